@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""BN254 G1 MSM benchmark on B200 (one JSON line on rank 0).
+
+Workload (step): one plain MSM over n = 2^22 affine points P_i = r_i * G
+(r_i uniform in Fr, seed 0) with uniform Fr scalars in Montgomery form,
+window c from the autotune table.  `value` = points/s with points and scalars
+resident in HBM (kernel-only, CUDA events on the launching stream, max over
+ranks); `e2e` = the same MSM through the reference-facing C ABI msm() with
+pinned host buffers (points and scalars copied in, the 64-byte result copied
+out, every step).  N > 1 GPUs run independent replicas (weak scaling).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl impeller|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BN254 MSM points/s at 2^22; batched vs per-call speedup; p50/p99 latency"
+UNIT = "points/s"
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sms, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sms.append(float(parts[0]))
+                maxs.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxs) if maxs else None,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+# ----------------------------------------------------------- algorithmics
+
+def signed_digit_stats(scalars_canonical: np.ndarray, c: int) -> tuple[int, int]:
+    """(nonzero signed digits, nonempty buckets) of the engine's recoding for
+    canonical scalars (n x 8 u32): the entry count of the accumulate phase."""
+    s = scalars_canonical.astype(np.uint64)
+    words = [s[:, 2 * k] | (s[:, 2 * k + 1] << np.uint64(32)) for k in range(4)]
+    W = math.ceil(254 / c)
+    half = 1 << (c - 1)
+    carry = np.zeros(s.shape[0], dtype=np.int64)
+    nonzero, buckets = 0, 0
+    for w in range(W):
+        o = w * c
+        k, sh = divmod(o, 64)
+        v = words[k] >> np.uint64(sh)
+        if sh + c > 64 and k + 1 < 4:
+            v |= words[k + 1] << np.uint64(64 - sh)
+        d = (v & np.uint64((1 << c) - 1)).astype(np.int64) + carry
+        if w + 1 < W:
+            neg = d >= half
+            mag = np.where(neg, (1 << c) - d, d)
+            carry = neg.astype(np.int64)
+        else:
+            mag = d
+        nz = mag != 0
+        nonzero += int(nz.sum())
+        buckets += int(np.unique(mag[nz]).size)
+    return nonzero, buckets
+
+
+# One Fq Montgomery product issues 8 rows x (8 lo + 8 hi for a*b[i], 1 for
+# the reduction factor, 8 lo + 8 hi for m*N) = 264 multiply-adds; a mixed
+# XYZZ + affine addition (madd-2008-s) is 10 products.
+IMAD_PER_MUL = 264
+MULS_PER_MADD = 10
+
+
+# ------------------------------------------------------------- reference
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU MSM (the C restatement of
+    core/tests/msm_halo2.rs best_multiexp; the Rust original cannot be built
+    here) on the box's host cores, on bounded samples of the 2^22 workload."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    n_full = 1 << args.log2n
+    sample = min(n_full, 1 << 18)
+    pts = O.gen_points(sample, seed=0, threads=cores)
+    scal = [O.gen_scalars(sample, seed=0, stream=1 + v, threads=cores) for v in range(2)]
+    for w in range(args.warmup):
+        O.msm(pts, scal[w % 2], threads=cores)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        O.msm(pts, scal[k % 2], threads=cores)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = sample / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (254-bit Montgomery)", "data": "synthetic (seeded r_i*G, uniform Fr)",
+        "config": {"workload": f"BN254 G1 MSM, n=2^{args.log2n} (each step a 2^18-point prefix on the CPU)",
+                   "threads": cores},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"2^18-point prefix of the 2^{args.log2n} workload per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ main
+
+def cpu_baseline(pts_host: np.ndarray, scal_host: np.ndarray) -> dict:
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    m = 1 << 16
+    t0 = time.perf_counter()
+    O.msm(pts_host[:m], scal_host[:m], threads=cores)
+    dt = time.perf_counter() - t0
+    # grow the sample to about 10 s of CPU work (at most 2^20 points)
+    while m < min(pts_host.shape[0], 1 << 20) and dt * 2.2 < 10.0:
+        m *= 2
+        t0 = time.perf_counter()
+        O.msm(pts_host[:m], scal_host[:m], threads=cores)
+        dt = time.perf_counter() - t0
+    return {"value": m / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first 2^{int(math.log2(m))} points/scalars of the workload, one MSM, {dt:.2f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="impeller", choices=["impeller", "reference"])
+    ap.add_argument("--log2n", type=int, default=22)
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e / batched / CPU legs")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", args.gpus if args.gpus else 1)
+    local = env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from impeller_b200 import msm as M
+    from impeller_b200 import lib as L
+    lib = L.load()
+    n = 1 << args.log2n
+    dev = local
+    stream = torch.cuda.current_stream()
+
+    pts = M.gen_points_device(n, seed=0, device=dev)
+    V = 4  # rotating scalar vectors: 4 x 128 MiB + 256 MiB of points, inputs > L2
+    scal = [M.gen_scalars_device(n, seed=0, stream_id=1 + v, device=dev) for v in range(V)]
+    ctx = M.MsmContext(pts, device=dev)
+    c = M.default_window(n)
+    outs = [torch.empty(16, dtype=torch.int32, device=f"cuda:{dev}") for _ in range(V)]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for w in range(args.warmup):
+        ctx.msm_device(scal[w % V], c=c, out=outs[w % V])
+    torch.cuda.synchronize()
+
+    lib.impeller_ctx_profile(ctx.handle, 1)
+    sampler = ClockSampler(dev)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        ctx.msm_device(scal[k % V], c=c, out=outs[k % V])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms_t = torch.tensor([ms], device=f"cuda:{dev}")
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * n / (ms_max / 1e3)
+
+    phases = (ctypes.c_double * 8)()
+    runs = ctypes.c_uint32()
+    L.check(lib.impeller_ctx_profile_read(ctx.handle, phases, 8, ctypes.byref(runs)))
+    lib.impeller_ctx_profile(ctx.handle, 0)
+    nr = max(1, runs.value)
+    phase_ms = {lib.impeller_phase_name(i).decode(): phases[i] / nr for i in range(8)}
+
+    line = None
+    if rank == 0:
+        # algorithmic work of the dominant kernel (accumulate) on the timed inputs
+        canon = [M.to_host(M.gen_scalars_device(n, seed=0, stream_id=1 + v, mont=False, device=dev)).reshape(n, 8)
+                 for v in range(V)]
+        stats = [signed_digit_stats(cv, c) for cv in canon]
+        madds = statistics.mean(nz - nb for nz, nb in stats)
+        entries = statistics.mean(nz for nz, _ in stats)
+        peak = ctypes.c_double()
+        L.check(lib.impeller_imad_peak(dev, ctypes.byref(peak)))
+        acc_ms = phase_ms["accumulate"]
+        achieved = madds * MULS_PER_MADD * IMAD_PER_MUL / (acc_ms * 1e-3) / 1e9
+        hbm_peak = None
+        try:
+            hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        except Exception:
+            hbm_peak = 6650.0
+        sort_ms = phase_ms["histogram"] + phase_ms["scan"] + phase_ms["scatter"]
+        sort_bytes = 2 * 32 * n + 4 * entries + 3 * 4 * (1 << (c - 1)) * math.ceil(254 / c)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 (254-bit Montgomery, 8x32-bit limbs)",
+            "data": "synthetic: P_i = r_i*G (r_i uniform Fr, seed 0), uniform Fr scalars (seeded streams)",
+            "config": {"workload": f"plain single BN254 G1 MSM, n=2^{args.log2n}, window c={c} (autotune table)",
+                       "n": n, "window": c, "parallelism": f"replicas x{world}",
+                       "l2": "inputs > L2: 256 MiB points + 4 rotating 128 MiB scalar vectors"},
+            "gpu_launches": args.steps * 10,
+            "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+            "roofline": {"bound": "imad", "kernel": "k_accumulate", "achieved": achieved, "peak": peak.value,
+                         "unit": "G int-multiply-adds/s", "frac": achieved / peak.value, "traffic": None,
+                         "per_launch": {"madds": madds, "imad_per_madd": MULS_PER_MADD * IMAD_PER_MUL,
+                                        "ms": acc_ms},
+                         "peak_source": "impeller_imad_peak: independent mad.lo/mad.hi chains, measured live"},
+            "roofline_sort": {"bound": "hbm", "kernels": "k_histogram+k_scan+k_scatter",
+                              "achieved": sort_bytes / (sort_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                              "frac": sort_bytes / (sort_ms * 1e-3) / 1e9 / hbm_peak,
+                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+            "clocks": clocks,
+        }
+
+    if not args.no_extras and rank == 0:
+        line["e2e"] = e2e_reference_abi(M, pts, scal[0], n, c, args)
+        line["e2e_resident_srs"] = e2e_resident(M, ctx, scal[0], n, c, args)
+        line["batched"] = batched_vs_per_call(M, ctx, dev, args)
+        pts_host = M.to_host(pts[: 1 << 20]).reshape(-1, 16)
+        sc_host = M.to_host(scal[0][: 1 << 20]).reshape(-1, 8)
+        line["cpu_baseline"] = cpu_baseline(pts_host, sc_host)
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def e2e_reference_abi(M, d_pts, d_scal, n, c, args) -> dict:
+    """The reference's calling convention: host points and scalars (pinned),
+    blocking msm() that uploads both, computes and returns the affine point."""
+    import torch
+    cfg = M.MsmConfig(window_size=c, target_window=math.ceil(254 / c))
+    op = M.MSM(cfg)
+    buf, keep = M.alloc_gpu_buffer(op.get_buffer_size(n)[0])
+    hp = torch.empty((n, 16), dtype=torch.int32, pin_memory=True)
+    hs = torch.empty((n, 8), dtype=torch.int32, pin_memory=True)
+    hp.copy_(d_pts.cpu())
+    hs.copy_(d_scal.cpu())
+    pts_np = hp.numpy().view(np.uint32)
+    sc_np = hs.numpy().view(np.uint32)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        op.run([pts_np], [sc_np], [buf])
+    steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        op.run([pts_np], [sc_np], [buf])
+    dt = (time.perf_counter() - t0) / steps
+    del keep
+    return {"value": n / dt, "unit": UNIT, "h2d_bytes_per_step": n * (64 + 32), "d2h_bytes_per_step": 64,
+            "ms_per_step": dt * 1e3, "api": f"msm() C ABI ({M.lib_name(cfg)}), pinned host buffers, wall clock"}
+
+
+def e2e_resident(M, ctx, d_scal, n, c, args) -> dict:
+    import torch
+    hs = torch.empty((n, 8), dtype=torch.int32, pin_memory=True)
+    hs.copy_(d_scal.cpu())
+    sc_np = hs.numpy().view(np.uint32)
+    for _ in range(2):
+        ctx.msm_host(sc_np, c=c)
+    steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.msm_host(sc_np, c=c)
+    dt = (time.perf_counter() - t0) / steps
+    return {"value": n / dt, "unit": UNIT, "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": 64,
+            "ms_per_step": dt * 1e3, "api": "impeller_msm_host (points resident), pinned scalars, wall clock"}
+
+
+def batched_vs_per_call(M, ctx, dev, args) -> dict:
+    """64 MSMs, sizes log-uniform in [2^10, 2^20] (seed 0), over prefixes of
+    the resident SRS: one batched CUDA-graph run vs 64 per-call MSMs."""
+    import torch
+    rng = np.random.default_rng(0)
+    sizes = [int(round(2 ** rng.uniform(10, 20))) for _ in range(64)]
+    scal = [M.gen_scalars_device(s, seed=0, stream_id=1000 + i, device=dev) for i, s in enumerate(sizes)]
+    total = sum(sizes)
+    b = ctx.batch(sizes, graph=True)
+    out = torch.empty((64, 16), dtype=torch.int32, device=f"cuda:{dev}")
+    outs = [torch.empty(16, dtype=torch.int32, device=f"cuda:{dev}") for _ in sizes]
+    st = torch.cuda.current_stream()
+    for _ in range(3):
+        b.run(scal, out=out)
+        for i, s in enumerate(sizes):
+            ctx.msm_device(scal[i], n=s, out=outs[i])
+    torch.cuda.synchronize()
+    reps = 5
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record(st)
+    for _ in range(reps):
+        b.run(scal, out=out)
+    e[1].record(st)
+    for _ in range(reps):
+        for i, s in enumerate(sizes):
+            ctx.msm_device(scal[i], n=s, out=outs[i])
+    e[2].record(st)
+    torch.cuda.synchronize()
+    tb = e[0].elapsed_time(e[1]) / reps
+    tp = e[1].elapsed_time(e[2]) / reps
+    same = bool(torch.equal(out, torch.stack(outs)))
+    launches = b.launches
+    b.close()
+    return {"workload": "64 MSMs, n log-uniform in [2^10, 2^20] (seed 0), prefixes of one resident SRS",
+            "total_points": total, "batched_ms": tb, "per_call_ms": tp,
+            "batched_points_per_s": total / (tb * 1e-3), "per_call_points_per_s": total / (tp * 1e-3),
+            "speedup": tp / tb, "results_identical": same, "launches_per_batch": launches,
+            "launches_per_call_total": 10 * len(sizes)}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,411 @@
+// The reference's C ABI, msm() and msm_precompute(), on the B200 engine.
+//
+// Semantics follow core/src/msm/src/msm.cu:9-49 and the classes it drives in
+// core/src/msm/src/msm_impl.cuh:
+//   - buffers == NULL: write the per-card scratch size and return
+//     (msm.cu:20-22, alloc_gpu at msm_impl.cuh:625-656);
+//   - the len points are split into num_cards equal ranges, one per card
+//     (MultiGPUMSM, msm_impl.cuh:832-844); each card splits its range into
+//     `parts` chunks that are uploaded and processed in turn (MSM::run,
+//     msm_impl.cuh:374-547), and runs `batch_per_run` scalar vectors per pass
+//     over the uploaded points (MSM::msm, msm_impl.cuh:735-749);
+//   - window j's points come from table j / n_windows (distribute_windows,
+//     msm_impl.cuh:56-68);
+//   - the result of each batch is written as a 16-word affine point in
+//     Montgomery form, identity (0,0) (msm.cu:37-39).
+// Unlike the reference, the per-part and per-card partial sums are added on
+// the device, and only the canonical affine result leaves the GPU.
+#include <algorithm>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/impeller_msm.h"
+#include "engine.h"
+
+using namespace impeller;
+
+namespace {
+
+#define CK(x)                                                                                   \
+    do {                                                                                        \
+        cudaError_t _e = (x);                                                                   \
+        if (_e != cudaSuccess) {                                                                \
+            set_error(std::string(#x) + " failed: " + cudaGetErrorString(_e));                  \
+            return _e;                                                                          \
+        }                                                                                       \
+    } while (0)
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct Config {
+    u32 c, W, n_windows, n_tables;
+    bool debug;
+};
+
+bool make_config(unsigned window_size, unsigned target_window, int debug, Config &cfg) {
+    if (window_size < 3 || window_size > 31) {
+        set_error("window_size must be in [3, 31]");
+        return false;
+    }
+    if (target_window == 0) {
+        set_error("target_window must be at least 1");
+        return false;
+    }
+    cfg.c = window_size;
+    cfg.W = digit_windows(window_size);
+    cfg.n_windows = std::min(cfg.W, target_window);
+    cfg.n_tables = (cfg.W + cfg.n_windows - 1) / cfg.n_windows;
+    cfg.debug = debug != 0;
+    return true;
+}
+
+// Per-card carve-out of the caller's buffer.
+struct CardLayout {
+    u64 card_off = 0, card_len = 0, part_len = 0;
+    size_t o_points = 0, o_scalars = 0, o_carry = 0, o_results = 0, o_combine = 0, o_plan = 0, bytes = 0;
+};
+
+std::vector<MsmShape> group_shapes(const Config &cfg, u32 M, u32 n, u32 part_len) {
+    std::vector<MsmShape> s(M, MsmShape{n, cfg.c, cfg.n_windows, part_len});
+    return s;
+}
+
+bool card_layout(const Config &cfg, int device, u64 len, u32 num_cards, u32 card, u32 parts, u32 batch_per_run,
+                 CardLayout &L, size_t &plan_bytes) {
+    const u64 per_card = (len + num_cards - 1) / num_cards;
+    L.card_off = std::min<u64>(len, (u64)card * per_card);
+    L.card_len = std::min<u64>(per_card, len - L.card_off);
+    L.part_len = (L.card_len + parts - 1) / parts;
+    if (L.part_len * cfg.n_tables >= (1ull << 31)) {
+        set_error("part length times window tables exceeds 2^31 points; raise `parts`");
+        return false;
+    }
+    plan_bytes = 0;
+    if (L.part_len) {
+        Plan p;
+        if (!Plan::build(p, device, group_shapes(cfg, batch_per_run, (u32)L.part_len, (u32)L.part_len))) return false;
+        plan_bytes = p.scratch_bytes();
+    }
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        size_t o = off;
+        off = align_up(off + b, 256);
+        return o;
+    };
+    L.o_points = take((size_t)cfg.n_tables * L.part_len * 64);
+    L.o_scalars = take((size_t)batch_per_run * L.part_len * 32);
+    L.o_carry = take((size_t)batch_per_run * 128);
+    L.o_results = take((size_t)batch_per_run * 64);
+    L.o_combine = take((size_t)num_cards * 128 + 64);
+    L.o_plan = take(plan_bytes);
+    L.bytes = off;
+    return true;
+}
+
+cudaStream_t device_stream(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaStream_t> streams;
+    std::lock_guard<std::mutex> g(mu);
+    auto it = streams.find(device);
+    if (it != streams.end()) return it->second;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    streams[device] = s;
+    return s;
+}
+
+struct CardJob {
+    const Config *cfg;
+    int device;
+    void *buffer;
+    CardLayout L;
+    u32 parts, batch_per_run, batches, num_cards;
+    unsigned int const *const *h_points;
+    unsigned int const *const *h_scalars;
+    unsigned int *const *h_result;        // single card: results written directly
+    std::vector<u32> partials;            // multi card: batches x 32 u32 (XYZZ)
+    cudaError_t status = cudaSuccess;
+    std::string error;
+};
+
+cudaError_t run_card(CardJob &J) {
+    const Config &cfg = *J.cfg;
+    CK(cudaSetDevice(J.device));
+    cudaStream_t st = device_stream(J.device);
+    if (!st) {
+        set_error("could not create a stream");
+        return cudaErrorUnknown;
+    }
+    unsigned char *base = static_cast<unsigned char *>(J.buffer);
+    u32 *d_points = reinterpret_cast<u32 *>(base + J.L.o_points);
+    u32 *d_scalars = reinterpret_cast<u32 *>(base + J.L.o_scalars);
+    u32 *d_carry = reinterpret_cast<u32 *>(base + J.L.o_carry);
+    u32 *d_results = reinterpret_cast<u32 *>(base + J.L.o_results);
+    void *plan_scratch = base + J.L.o_plan;
+    const bool multi = J.num_cards > 1;
+    if (multi) J.partials.assign((size_t)J.batches * 32, 0);
+
+    std::map<std::pair<u32, u32>, std::unique_ptr<Plan>> plans;
+    auto get_plan = [&](u32 M, u32 n) -> Plan * {
+        auto key = std::make_pair(M, n);
+        auto it = plans.find(key);
+        if (it != plans.end()) return it->second.get();
+        std::unique_ptr<Plan> p(new Plan());
+        if (!Plan::build(*p, J.device, group_shapes(cfg, M, n, (u32)J.L.part_len))) return nullptr;
+        Plan *raw = p.get();
+        plans[key] = std::move(p);
+        return raw;
+    };
+
+    bool points_resident = false;
+    for (u32 g = 0; g < J.batches; g += J.batch_per_run) {
+        const u32 M = std::min(J.batch_per_run, J.batches - g);
+        if (J.L.card_len == 0) {
+            // an empty range contributes the identity
+            if (!multi)
+                for (u32 b = 0; b < M; b++) std::fill(J.h_result[g + b], J.h_result[g + b] + 16, 0u);
+            continue;
+        }
+        CK(cudaMemsetAsync(d_carry, 0, (size_t)M * 128, st));
+        for (u32 p = 0; p < J.parts; p++) {
+            const u64 off = (u64)p * J.L.part_len;
+            if (off >= J.L.card_len) break;
+            const u64 cur = std::min<u64>(J.L.part_len, J.L.card_len - off);
+            const bool last = off + cur >= J.L.card_len;
+            if (!(points_resident && J.parts == 1)) {
+                for (u32 t = 0; t < cfg.n_tables; t++)
+                    CK(cudaMemcpyAsync(d_points + (size_t)t * J.L.part_len * 16,
+                                       J.h_points[t] + (J.L.card_off + off) * 16, cur * 64, cudaMemcpyHostToDevice,
+                                       st));
+                points_resident = true;
+            }
+            std::vector<const u32 *> sc(M);
+            for (u32 b = 0; b < M; b++) {
+                CK(cudaMemcpyAsync(d_scalars + (size_t)b * J.L.part_len * 8, J.h_scalars[g + b] + (J.L.card_off + off) * 8,
+                                   cur * 32, cudaMemcpyHostToDevice, st));
+                sc[b] = d_scalars + (size_t)b * J.L.part_len * 8;
+            }
+            Plan *plan = get_plan(M, (u32)cur);
+            if (!plan) return cudaErrorInvalidValue;
+            const int mode = (last && !multi) ? 1 : 2;
+            cudaEvent_t t0 = nullptr, t1 = nullptr;
+            if (cfg.debug) {
+                cudaEventCreate(&t0);
+                cudaEventCreate(&t1);
+                cudaEventRecord(t0, st);
+            }
+            cudaError_t e = plan->enqueue(plan_scratch, d_points, sc.data(), d_results, mode, st, d_carry);
+            if (e != cudaSuccess) return e;
+            if (cfg.debug) {
+                cudaEventRecord(t1, st);
+                cudaEventSynchronize(t1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, t0, t1);
+                std::fprintf(stderr, "impeller msm: card %d group %u part %u n=%llu batch=%u: %.3f ms\n", J.device, g,
+                             p, (unsigned long long)cur, M, ms);
+                cudaEventDestroy(t0);
+                cudaEventDestroy(t1);
+            }
+        }
+        if (!multi) {
+            for (u32 b = 0; b < M; b++)
+                CK(cudaMemcpyAsync(J.h_result[g + b], d_results + (size_t)b * 16, 64, cudaMemcpyDeviceToHost, st));
+        } else {
+            CK(cudaMemcpyAsync(J.partials.data() + (size_t)g * 32, d_carry, (size_t)M * 128, cudaMemcpyDeviceToHost,
+                               st));
+        }
+        CK(cudaStreamSynchronize(st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+unsigned int impeller_msm_n_precompute(unsigned int window_size, unsigned int target_window) {
+    Config cfg;
+    if (!make_config(window_size, target_window, 0, cfg)) return 0;
+    return cfg.n_tables;
+}
+
+cudaError_t impeller_msm_cfg(unsigned int window_size, unsigned int target_window, int debug, void *const *buffers,
+                             unsigned long *buffer_sizes, unsigned long long len, unsigned int batch_per_run,
+                             unsigned int parts, unsigned int stage_scalers, unsigned int stage_points,
+                             unsigned int num_cards, const unsigned int *cards, unsigned int const *const *h_points,
+                             unsigned int batches, unsigned int const *const *h_scaler_batch,
+                             unsigned int *const *h_result) {
+    (void)stage_scalers;
+    (void)stage_points;
+    Config cfg;
+    if (!make_config(window_size, target_window, debug, cfg)) return cudaErrorInvalidValue;
+    if (num_cards == 0 || !cards) {
+        set_error("msm: at least one card is required");
+        return cudaErrorInvalidValue;
+    }
+    if (parts == 0 || batch_per_run == 0) {
+        set_error("msm: parts and batch_per_run must be at least 1");
+        return cudaErrorInvalidValue;
+    }
+    std::vector<CardLayout> layouts(num_cards);
+    for (u32 i = 0; i < num_cards; i++) {
+        size_t pb = 0;
+        if (!card_layout(cfg, (int)cards[i], len, num_cards, i, parts, batch_per_run, layouts[i], pb))
+            return cudaErrorInvalidValue;
+    }
+    if (buffers == nullptr) {
+        if (!buffer_sizes) {
+            set_error("msm: size query needs buffer_sizes");
+            return cudaErrorInvalidValue;
+        }
+        for (u32 i = 0; i < num_cards; i++) buffer_sizes[i] = (unsigned long)layouts[i].bytes;
+        return cudaSuccess;
+    }
+    if (batches == 0) return cudaSuccess;
+    if (!h_points || !h_scaler_batch || !h_result) {
+        set_error("msm: null host array");
+        return cudaErrorInvalidValue;
+    }
+    for (u32 t = 0; t < cfg.n_tables; t++)
+        if (!h_points[t] && len) {
+            set_error("msm: missing window table pointer");
+            return cudaErrorInvalidValue;
+        }
+    for (u32 b = 0; b < batches; b++)
+        if ((!h_scaler_batch[b] && len) || !h_result[b]) {
+            set_error("msm: missing scalar or result pointer");
+            return cudaErrorInvalidValue;
+        }
+
+    std::vector<CardJob> jobs(num_cards);
+    for (u32 i = 0; i < num_cards; i++) {
+        CardJob &J = jobs[i];
+        J.cfg = &cfg;
+        J.device = (int)cards[i];
+        J.buffer = buffers[i];
+        J.L = layouts[i];
+        J.parts = parts;
+        J.batch_per_run = batch_per_run;
+        J.batches = batches;
+        J.num_cards = num_cards;
+        J.h_points = h_points;
+        J.h_scalars = h_scaler_batch;
+        J.h_result = h_result;
+    }
+    if (num_cards == 1) {
+        return run_card(jobs[0]);
+    }
+    std::vector<std::thread> threads;
+    for (u32 i = 0; i < num_cards; i++)
+        threads.emplace_back([&jobs, i]() {
+            jobs[i].status = run_card(jobs[i]);
+            if (jobs[i].status != cudaSuccess) jobs[i].error = impeller::last_error();
+        });
+    for (auto &t : threads) t.join();
+    for (auto &J : jobs)
+        if (J.status != cudaSuccess) {
+            set_error(J.error);
+            return J.status;
+        }
+    // one exchange: each card's XYZZ partial to card 0, summed there
+    CK(cudaSetDevice((int)cards[0]));
+    cudaStream_t st = device_stream((int)cards[0]);
+    unsigned char *base0 = static_cast<unsigned char *>(buffers[0]);
+    u32 *d_comb = reinterpret_cast<u32 *>(base0 + layouts[0].o_combine);
+    u32 *d_out = d_comb + (size_t)num_cards * 32;
+    std::vector<u32> gather((size_t)num_cards * 32);
+    for (u32 b = 0; b < batches; b++) {
+        for (u32 i = 0; i < num_cards; i++)
+            std::copy(jobs[i].partials.begin() + (size_t)b * 32, jobs[i].partials.begin() + (size_t)(b + 1) * 32,
+                      gather.begin() + (size_t)i * 32);
+        CK(cudaMemcpyAsync(d_comb, gather.data(), gather.size() * 4, cudaMemcpyHostToDevice, st));
+        cudaError_t e = combine_xyzz(d_comb, num_cards, d_out, st);
+        if (e != cudaSuccess) return e;
+        CK(cudaMemcpyAsync(h_result[b], d_out, 64, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    return cudaSuccess;
+}
+
+cudaError_t impeller_msm_precompute_cfg(unsigned int window_size, unsigned int target_window,
+                                        unsigned long long len, unsigned int *const *h_points,
+                                        unsigned int max_cards) {
+    Config cfg;
+    if (!make_config(window_size, target_window, 0, cfg)) return cudaErrorInvalidValue;
+    if (cfg.n_tables == 1 || len == 0) return cudaSuccess;
+    if (!h_points) {
+        set_error("msm_precompute: null h_points");
+        return cudaErrorInvalidValue;
+    }
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    const int devices = std::max(1, std::min(ndev, (int)std::max(1u, max_cards)));
+    const u64 per = (len + devices - 1) / devices;
+    const u32 shift = cfg.n_windows * cfg.c;
+    std::vector<cudaError_t> status(devices, cudaSuccess);
+    std::vector<std::string> errs(devices);
+    auto work = [&](int dev) -> cudaError_t {
+        const u64 off = std::min<u64>(len, (u64)dev * per);
+        const u64 cnt = std::min<u64>(per, len - off);
+        if (cnt == 0) return cudaSuccess;
+        CK(cudaSetDevice(dev));
+        cudaStream_t st = device_stream(dev);
+        const u64 chunk = std::min<u64>(cnt, 1ull << 20);
+        u32 *d = nullptr;
+        CK(cudaMalloc(&d, (size_t)cfg.n_tables * chunk * 64));
+        cudaError_t e = cudaSuccess;
+        for (u64 s = 0; s < cnt && e == cudaSuccess; s += chunk) {
+            const u64 m = std::min<u64>(chunk, cnt - s);
+            e = cudaMemcpyAsync(d, h_points[0] + (off + s) * 16, m * 64, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = precompute_tables(d, m, shift, cfg.n_tables, st);
+            for (u32 t = 1; t < cfg.n_tables && e == cudaSuccess; t++)
+                e = cudaMemcpyAsync(h_points[t] + (off + s) * 16, d + (size_t)t * m * 16, m * 64,
+                                    cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        }
+        cudaFree(d);
+        if (e != cudaSuccess) set_error(std::string("msm_precompute: ") + cudaGetErrorString(e));
+        return e;
+    };
+    std::vector<std::thread> th;
+    for (int d = 0; d < devices; d++)
+        th.emplace_back([&, d]() {
+            status[d] = work(d);
+            if (status[d] != cudaSuccess) errs[d] = impeller::last_error();
+        });
+    for (auto &t : th) t.join();
+    for (int d = 0; d < devices; d++)
+        if (status[d] != cudaSuccess) {
+            set_error(errs[d]);
+            return status[d];
+        }
+    return cudaSuccess;
+}
+
+#ifndef IMPELLER_DEFAULT_WINDOW
+#define IMPELLER_DEFAULT_WINDOW 16
+#endif
+#ifndef IMPELLER_DEFAULT_TARGET
+#define IMPELLER_DEFAULT_TARGET 16
+#endif
+
+cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, unsigned long long len, unsigned int batch_per_run,
+                unsigned int parts, unsigned int stage_scalers, unsigned int stage_points, unsigned int num_cards,
+                const unsigned int *cards, unsigned int const *const *h_points, unsigned int batches,
+                unsigned int const *const *h_scaler_batch, unsigned int *const *h_result) {
+    return impeller_msm_cfg(IMPELLER_DEFAULT_WINDOW, IMPELLER_DEFAULT_TARGET, 0, buffers, buffer_sizes, len,
+                            batch_per_run, parts, stage_scalers, stage_points, num_cards, cards, h_points, batches,
+                            h_scaler_batch, h_result);
+}
+
+cudaError_t msm_precompute(unsigned long long len, unsigned int *const *h_points, unsigned int max_cards) {
+    return impeller_msm_precompute_cfg(IMPELLER_DEFAULT_WINDOW, IMPELLER_DEFAULT_TARGET, len, h_points, max_cards);
+}
+
+}  // extern "C"

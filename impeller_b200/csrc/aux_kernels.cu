@@ -1,0 +1,283 @@
+// Seeded synthetic inputs on the device, and element-wise field / point
+// operations exported for the parity tests.
+//
+// The generator definitions are the ones the CPU oracle uses (splitmix64
+// counter streams; uniform Fr element i = (lo + hi * 2^256) mod r from words
+// 8i..8i+7; the skewed mix; P_i = r_i * G with G = (1, 2)), so the device and
+// the oracle produce the same inputs bit for bit.
+#include <string>
+
+#include "../../include/impeller_msm.h"
+#include "bn254.cuh"
+#include "engine.h"
+
+using namespace bn254;
+
+namespace {
+
+#define GAMMA 0x9e3779b97f4a7c15ull
+
+__device__ __forceinline__ u64 mix64(u64 z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ u64 stream_key(u64 seed, u64 stream) {
+    return mix64(seed * GAMMA + mix64(stream + 0x632be59bd9b4e019ull));
+}
+
+__device__ __forceinline__ u64 stream_word(u64 key, u64 idx) { return mix64(key + (idx + 1) * GAMMA); }
+
+__device__ __forceinline__ bool geq_r(const u32 x[8]) {
+    const u32 m[8] = {FrP::M0, FrP::M1, FrP::M2, FrP::M3, FrP::M4, FrP::M5, FrP::M6, FrP::M7};
+    for (int i = 7; i >= 0; i--)
+        if (x[i] != m[i]) return x[i] > m[i];
+    return true;
+}
+
+__device__ __forceinline__ void sub_r(u32 x[8]) {
+    const u32 m[8] = {FrP::M0, FrP::M1, FrP::M2, FrP::M3, FrP::M4, FrP::M5, FrP::M6, FrP::M7};
+    u64 borrow = 0;
+    for (int i = 0; i < 8; i++) {
+        u64 d = (u64)x[i] - m[i] - borrow;
+        x[i] = (u32)d;
+        borrow = (d >> 63) & 1;
+    }
+}
+
+__device__ __forceinline__ Fr fr_r2() {
+    Fr r;
+    r.l[0] = 0xae216da7u; r.l[1] = 0x1bb8e645u; r.l[2] = 0xe35c59e3u; r.l[3] = 0x53fe3ab1u;
+    r.l[4] = 0x53bb8085u; r.l[5] = 0x8c49833du; r.l[6] = 0x7f4e44a5u; r.l[7] = 0x0216d0b1u;
+    return r;
+}
+
+__device__ __forceinline__ Fq fq_r2() {
+    Fq r;
+    r.l[0] = 0x538afa89u; r.l[1] = 0xf32cfc5bu; r.l[2] = 0xd44501fbu; r.l[3] = 0xb5e71911u;
+    r.l[4] = 0x0a417ff6u; r.l[5] = 0x47ab1effu; r.l[6] = 0xcab8351fu; r.l[7] = 0x06d89f71u;
+    return r;
+}
+
+// canonical uniform Fr element idx of the stream with this key
+__device__ Fr uniform_fr(u64 key, u64 idx) {
+    u32 lo[8], hi[8];
+    for (int k = 0; k < 4; k++) {
+        u64 w = stream_word(key, 8 * idx + k);
+        lo[2 * k] = (u32)w;
+        lo[2 * k + 1] = (u32)(w >> 32);
+        u64 v = stream_word(key, 8 * idx + 4 + k);
+        hi[2 * k] = (u32)v;
+        hi[2 * k + 1] = (u32)(v >> 32);
+    }
+    while (geq_r(lo)) sub_r(lo);
+    while (geq_r(hi)) sub_r(hi);
+    Fr h, l;
+    for (int i = 0; i < 8; i++) {
+        h.l[i] = hi[i];
+        l.l[i] = lo[i];
+    }
+    Fr t = fe_mul<FrP>(h, fr_r2());  // hi * 2^256 mod r
+    return fe_add<FrP>(l, t);
+}
+
+__global__ void k_gen_scalars(u32 *out, u64 n, u64 seed, u64 stream, int dist, u64 start, int mont) {
+    const u64 key = stream_key(seed, stream);
+    const u64 key_cat = stream_key(seed, stream + (1ull << 32));
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 idx = start + i;
+        Fr v = fe_zero<FrP>();
+        bool uniform = true;
+        if (dist == 1) {
+            u64 u = stream_word(key_cat, idx);
+            u64 cat = u % 10;
+            if (cat < 7) {
+                uniform = false;
+                if (cat >= 2 && cat < 4) v.l[0] = 1;
+                else if (cat >= 4) v.l[0] = (u32)((u >> 40) & 0xffffu);
+            }
+        }
+        if (uniform) v = uniform_fr(key, idx);
+        if (mont) v = fe_mul<FrP>(v, fr_r2());
+        fe_store(out + 8 * i, v);
+    }
+}
+
+__global__ void k_gen_points(u32 *out, u64 n, u64 seed, u64 start) {
+    const u64 key = stream_key(seed, 0);
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        Fr r = uniform_fr(key, start + i);
+        Affine g;
+        g.x = fe_one<FqP>();
+        g.y = fe_add<FqP>(g.x, g.x);
+        Xyzz acc = xyzz_identity();
+        for (int bit = 255; bit >= 0; bit--) {
+            acc = xyzz_dbl(acc);
+            if ((r.l[bit >> 5] >> (bit & 31)) & 1u) acc = xyzz_add_affine(acc, g);
+        }
+        affine_store(out + 16 * i, xyzz_to_affine(acc));
+    }
+}
+
+template <class F>
+__device__ Fe<F> test_op(int op, const Fe<F> &a, const Fe<F> &b, const Fe<F> &r2) {
+    switch (op) {
+    case 0: return fe_add<F>(a, b);
+    case 1: return fe_sub<F>(a, b);
+    case 2: return fe_mul<F>(a, b);
+    case 3: return fe_sqr<F>(a);
+    case 4: return fe_neg<F>(a);
+    case 5: return fe_mul<F>(a, r2);
+    case 6: return fe_from_mont<F>(a);
+    case 7: return fe_inv<F>(a);
+    default: return fe_pow<F>(a, b.l);
+    }
+}
+
+__global__ void k_test_field(int field, int op, const u32 *a, const u32 *b, u32 *out, u64 count) {
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    if (field == 0) {
+        Fq x = fe_load<FqP>(a + 8 * i), y = b ? fe_load<FqP>(b + 8 * i) : fe_zero<FqP>();
+        fe_store(out + 8 * i, test_op<FqP>(op, x, y, fq_r2()));
+    } else {
+        Fr x = fe_load<FrP>(a + 8 * i), y = b ? fe_load<FrP>(b + 8 * i) : fe_zero<FrP>();
+        fe_store(out + 8 * i, test_op<FrP>(op, x, y, fr_r2()));
+    }
+}
+
+__global__ void k_test_point(int op, const u32 *p, const u32 *q, u32 *out, u64 count) {
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    Affine a = affine_load(p + 16 * i);
+    Xyzz r;
+    switch (op) {
+    case 0: r = xyzz_add_affine(xyzz_from_affine(a), affine_load(q + 16 * i)); break;
+    case 1: r = xyzz_dbl(xyzz_from_affine(a)); break;
+    case 2: r = xyzz_add(xyzz_from_affine(a), xyzz_from_affine(affine_load(q + 16 * i))); break;
+    default: {
+        const u32 *k = q + 8 * i;
+        Xyzz acc = xyzz_identity();
+        for (int bit = 255; bit >= 0; bit--) {
+            acc = xyzz_dbl(acc);
+            if ((k[bit >> 5] >> (bit & 31)) & 1u) acc = xyzz_add_affine(acc, a);
+        }
+        r = acc;
+    }
+    }
+    affine_store(out + 16 * i, xyzz_to_affine(r));
+}
+
+// 16 independent accumulators per thread: 8 mad.lo and 8 mad.hi per step.
+__global__ void k_imad_peak(u32 *out, u32 iters, u32 seed) {
+    u32 a[8], lo[8], hi[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        a[k] = seed * (threadIdx.x + 3 * k + 1) + blockIdx.x;
+        lo[k] = a[k] ^ 0x5bd1e995u;
+        hi[k] = a[k] + 0x9e3779b9u;
+    }
+#pragma unroll 1
+    for (u32 it = 0; it < iters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            asm volatile("mad.lo.u32 %0, %1, %2, %0;" : "+r"(lo[k]) : "r"(a[k]), "r"(a[(k + 1) & 7]));
+            asm volatile("mad.hi.u32 %0, %1, %2, %0;" : "+r"(hi[k]) : "r"(a[k]), "r"(a[(k + 3) & 7]));
+        }
+    }
+    u32 x = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) x ^= lo[k] ^ hi[k];
+    if (x == 0x12345678u) out[blockIdx.x * blockDim.x + threadIdx.x] = x;
+}
+
+cudaError_t launched(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) impeller::set_error(std::string("launch of ") + what + " failed: " + cudaGetErrorString(e));
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+cudaError_t impeller_gen_scalars(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t stream, int dist,
+                                 uint64_t start, int mont, cudaStream_t s) {
+    if (!d_out && n) {
+        impeller::set_error("impeller_gen_scalars: null output");
+        return cudaErrorInvalidValue;
+    }
+    if (n == 0) return cudaSuccess;
+    const u64 blocks = (n + 255) / 256;
+    k_gen_scalars<<<(unsigned)(blocks < 65535 ? blocks : 65535), 256, 0, s>>>(d_out, n, seed, stream, dist, start,
+                                                                               mont);
+    return launched("k_gen_scalars");
+}
+
+cudaError_t impeller_gen_points(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t start, cudaStream_t s) {
+    if (!d_out && n) {
+        impeller::set_error("impeller_gen_points: null output");
+        return cudaErrorInvalidValue;
+    }
+    if (n == 0) return cudaSuccess;
+    const u64 blocks = (n + 127) / 128;
+    k_gen_points<<<(unsigned)(blocks < 65535 ? blocks : 65535), 128, 0, s>>>(d_out, n, seed, start);
+    return launched("k_gen_points");
+}
+
+cudaError_t impeller_imad_peak(int device, double *gops) {
+    if (!gops) return cudaErrorInvalidValue;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return e;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const u32 blocks = (u32)sms * 8, threads = 256, iters = 1u << 14;
+    u32 *out = nullptr;
+    if ((e = cudaMalloc(&out, (size_t)blocks * threads * 4)) != cudaSuccess) return e;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    k_imad_peak<<<blocks, threads>>>(out, iters / 8, 7u);  // warm-up
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; rep++) {
+        cudaEventRecord(t0);
+        k_imad_peak<<<blocks, threads>>>(out, iters, 7u);
+        cudaEventRecord(t1);
+        cudaEventSynchronize(t1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t0, t1);
+        best = ms < best ? ms : best;
+    }
+    e = cudaGetLastError();
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaFree(out);
+    if (e != cudaSuccess) return e;
+    *gops = (double)blocks * threads * iters * 16.0 / (best * 1e-3) / 1e9;
+    return cudaSuccess;
+}
+
+cudaError_t impeller_test_field_op(int field, int op, const uint32_t *d_a, const uint32_t *d_b, uint32_t *d_out,
+                                   uint64_t count, cudaStream_t s) {
+    if (field < 0 || field > 1 || op < 0 || op > 8 || !d_a || !d_out) {
+        impeller::set_error("impeller_test_field_op: bad argument");
+        return cudaErrorInvalidValue;
+    }
+    if (count == 0) return cudaSuccess;
+    k_test_field<<<(unsigned)((count + 127) / 128), 128, 0, s>>>(field, op, d_a, d_b, d_out, count);
+    return launched("k_test_field");
+}
+
+cudaError_t impeller_test_point_op(int op, const uint32_t *d_p, const uint32_t *d_q, uint32_t *d_out,
+                                   uint64_t count, cudaStream_t s) {
+    if (op < 0 || op > 3 || !d_p || !d_out || (op != 1 && !d_q)) {
+        impeller::set_error("impeller_test_point_op: bad argument");
+        return cudaErrorInvalidValue;
+    }
+    if (count == 0) return cudaSuccess;
+    k_test_point<<<(unsigned)((count + 127) / 128), 128, 0, s>>>(op, d_p, d_q, d_out, count);
+    return launched("k_test_point");
+}
+
+}  // extern "C"

@@ -1,0 +1,531 @@
+// BN254 field and G1 arithmetic for sm_100a.
+//
+// Field elements are 8 little-endian 32-bit limbs in Montgomery form with
+// R = 2^256, the layout of the reference's mont::Element
+// (core/src/common/mont/src/field.cuh:906-1204) and of its C ABI.
+// Multiplication is coarsely integrated operand scanning on the integer
+// multiply pipe: per row, one carry chain of mad.lo and one of mad.hi for
+// a*b[i], one mul for the reduction factor, and one lo and one hi chain for
+// m*N.  Because N < 2^254, the running value stays below 3N < 2^256 even for
+// inputs in [0, 2N), so nine words hold every intermediate and no carry ever
+// leaves word 8.
+//
+// Curve points use XYZZ coordinates (x = X/ZZ, y = Y/ZZZ, ZZ^3 = ZZZ^2), the
+// point representation of core/src/common/curve/src/curve_xyzz.cuh:252-418,
+// with the Explicit-Formulas Database's madd-2008-s, add-2008-s,
+// dbl-2008-s-1 and mdbl-2008-s-1 for a = 0 (y^2 = x^3 + 3,
+// core/src/common/curve/src/bn254.cuh:13-31).  ZZ == 0 marks the identity;
+// an affine point with y == 0 is the identity (curve_xyzz.cuh:204-210).
+#pragma once
+
+#include <cstdint>
+
+namespace bn254 {
+
+typedef uint32_t u32;
+typedef uint64_t u64;
+
+struct FqP {
+    static constexpr u32 M0 = 0xd87cfd47u, M1 = 0x3c208c16u, M2 = 0x6871ca8du, M3 = 0x97816a91u;
+    static constexpr u32 M4 = 0x8181585du, M5 = 0xb85045b6u, M6 = 0xe131a029u, M7 = 0x30644e72u;
+    static constexpr u32 INV = 0xe4866389u;  // -p^{-1} mod 2^32
+    // R mod p (Montgomery one)
+    static constexpr u32 R0 = 0xc58f0d9du, R1 = 0xd35d438du, R2 = 0xf5c70b3du, R3 = 0x0a78eb28u;
+    static constexpr u32 R4 = 0x7879462cu, R5 = 0x666ea36fu, R6 = 0x9a07df2fu, R7 = 0x0e0a77c1u;
+};
+
+struct FrP {
+    static constexpr u32 M0 = 0xf0000001u, M1 = 0x43e1f593u, M2 = 0x79b97091u, M3 = 0x2833e848u;
+    static constexpr u32 M4 = 0x8181585du, M5 = 0xb85045b6u, M6 = 0xe131a029u, M7 = 0x30644e72u;
+    static constexpr u32 INV = 0xefffffffu;  // -r^{-1} mod 2^32
+    static constexpr u32 R0 = 0x4ffffffbu, R1 = 0xac96341cu, R2 = 0x9f60cd29u, R3 = 0x36fc7695u;
+    static constexpr u32 R4 = 0x7879462eu, R5 = 0x666ea36fu, R6 = 0x9a07df2fu, R7 = 0x0e0a77c1u;
+};
+
+template <class F>
+struct Fe {
+    u32 l[8];
+};
+
+typedef Fe<FqP> Fq;
+typedef Fe<FrP> Fr;
+
+template <class F>
+__host__ __device__ __forceinline__ Fe<F> fe_zero() {
+    Fe<F> r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.l[i] = 0;
+    return r;
+}
+
+template <class F>
+__host__ __device__ __forceinline__ Fe<F> fe_one() {
+    Fe<F> r;
+    r.l[0] = F::R0; r.l[1] = F::R1; r.l[2] = F::R2; r.l[3] = F::R3;
+    r.l[4] = F::R4; r.l[5] = F::R5; r.l[6] = F::R6; r.l[7] = F::R7;
+    return r;
+}
+
+template <class F>
+__device__ __forceinline__ bool fe_is_zero(const Fe<F> &a) {
+    u32 x = (a.l[0] | a.l[1]) | (a.l[2] | a.l[3]) | (a.l[4] | a.l[5]) | (a.l[6] | a.l[7]);
+    return x == 0;
+}
+
+template <class F>
+__device__ __forceinline__ bool fe_eq(const Fe<F> &a, const Fe<F> &b) {
+    u32 x = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) x |= a.l[i] ^ b.l[i];
+    return x == 0;
+}
+
+// r = (t < N) ? t : t - N, for t < 2N.
+template <class F>
+__device__ __forceinline__ void fe_reduce_once(Fe<F> &r, const u32 t[8]) {
+    u32 d[8], bw;
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+          "=r"(bw)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]),
+          "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5), "n"(F::M6), "n"(F::M7));
+    // bw == 0xffffffff when t < N: keep t
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.l[i] = bw ? t[i] : d[i];
+}
+
+// One CIOS row: t += a * bi; m = t0 * INV; t += m * N; t >>= 32.
+// t holds 9 words on entry (t[8] small) and on exit.
+#define BN_ROW(F, t, a, bi)                                                                              \
+    do {                                                                                                 \
+        u32 _m;                                                                                          \
+        asm("mad.lo.cc.u32  %0, %9,  %17, %0;\n\t"                                                       \
+            "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"                                                       \
+            "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"                                                       \
+            "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"                                                       \
+            "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"                                                       \
+            "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"                                                       \
+            "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"                                                       \
+            "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"                                                       \
+            "addc.u32       %8, %8, 0;\n\t"                                                              \
+            "mad.hi.cc.u32  %1, %9,  %17, %1;\n\t"                                                       \
+            "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"                                                       \
+            "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"                                                       \
+            "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"                                                       \
+            "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"                                                       \
+            "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"                                                       \
+            "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"                                                       \
+            "madc.hi.u32    %8, %16, %17, %8;"                                                           \
+            : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),     \
+              "+r"(t[7]), "+r"(t[8])                                                                     \
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),  \
+              "r"(bi));                                                                                  \
+        _m = t[0] * F::INV;                                                                              \
+        asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"                                                        \
+            "madc.lo.cc.u32 %1, %9, %11, %1;\n\t"                                                        \
+            "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"                                                        \
+            "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"                                                        \
+            "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"                                                        \
+            "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"                                                        \
+            "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"                                                        \
+            "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"                                                        \
+            "addc.u32       %8, %8, 0;\n\t"                                                              \
+            "mad.hi.cc.u32  %1, %9, %10, %1;\n\t"                                                        \
+            "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"                                                        \
+            "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"                                                        \
+            "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"                                                        \
+            "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"                                                        \
+            "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"                                                        \
+            "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"                                                        \
+            "madc.hi.u32    %8, %9, %17, %8;"                                                            \
+            : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),     \
+              "+r"(t[7]), "+r"(t[8])                                                                     \
+            : "r"(_m), "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5),         \
+              "n"(F::M6), "n"(F::M7));                                                                   \
+        t[0] = t[1]; t[1] = t[2]; t[2] = t[3]; t[3] = t[4];                                              \
+        t[4] = t[5]; t[5] = t[6]; t[6] = t[7]; t[7] = t[8]; t[8] = 0;                                    \
+    } while (0)
+
+// Montgomery product a*b*R^{-1} mod N, fully reduced (inputs reduced).
+template <class F>
+__device__ __forceinline__ Fe<F> fe_mul(const Fe<F> &a, const Fe<F> &b) {
+    u32 t[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) BN_ROW(F, t, a.l, b.l[i]);
+    Fe<F> r;
+    fe_reduce_once<F>(r, t);
+    return r;
+}
+
+template <class F>
+__device__ __forceinline__ Fe<F> fe_sqr(const Fe<F> &a) {
+    return fe_mul<F>(a, a);
+}
+
+// Leave Montgomery form: a * R^{-1} mod N (Montgomery reduction only).
+template <class F>
+__device__ __forceinline__ Fe<F> fe_from_mont(const Fe<F> &a) {
+    u32 t[9];
+#pragma unroll
+    for (int i = 0; i < 8; i++) t[i] = a.l[i];
+    t[8] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        u32 m = t[0] * F::INV;
+        asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"
+            "madc.lo.cc.u32 %1, %9, %11, %1;\n\t"
+            "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"
+            "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"
+            "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"
+            "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"
+            "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"
+            "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"
+            "addc.u32       %8, %8, 0;\n\t"
+            "mad.hi.cc.u32  %1, %9, %10, %1;\n\t"
+            "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"
+            "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"
+            "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"
+            "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"
+            "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"
+            "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"
+            "madc.hi.u32    %8, %9, %17, %8;"
+            : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7]),
+              "+r"(t[8])
+            : "r"(m), "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5), "n"(F::M6),
+              "n"(F::M7));
+#pragma unroll
+        for (int k = 0; k < 8; k++) t[k] = t[k + 1];
+        t[8] = 0;
+    }
+    Fe<F> r;
+    fe_reduce_once<F>(r, t);
+    return r;
+}
+
+template <class F>
+__device__ __forceinline__ Fe<F> fe_add(const Fe<F> &a, const Fe<F> &b) {
+    u32 s[8];
+    asm("add.cc.u32  %0, %8, %16;\n\t"
+        "addc.cc.u32 %1, %9, %17;\n\t"
+        "addc.cc.u32 %2, %10, %18;\n\t"
+        "addc.cc.u32 %3, %11, %19;\n\t"
+        "addc.cc.u32 %4, %12, %20;\n\t"
+        "addc.cc.u32 %5, %13, %21;\n\t"
+        "addc.cc.u32 %6, %14, %22;\n\t"
+        "addc.u32    %7, %15, %23;"
+        : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]), "=r"(s[7])
+        : "r"(a.l[0]), "r"(a.l[1]), "r"(a.l[2]), "r"(a.l[3]), "r"(a.l[4]), "r"(a.l[5]), "r"(a.l[6]),
+          "r"(a.l[7]), "r"(b.l[0]), "r"(b.l[1]), "r"(b.l[2]), "r"(b.l[3]), "r"(b.l[4]), "r"(b.l[5]),
+          "r"(b.l[6]), "r"(b.l[7]));
+    Fe<F> r;
+    fe_reduce_once<F>(r, s);
+    return r;
+}
+
+template <class F>
+__device__ __forceinline__ Fe<F> fe_sub(const Fe<F> &a, const Fe<F> &b) {
+    u32 d[8], bw;
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+          "=r"(bw)
+        : "r"(a.l[0]), "r"(a.l[1]), "r"(a.l[2]), "r"(a.l[3]), "r"(a.l[4]), "r"(a.l[5]), "r"(a.l[6]),
+          "r"(a.l[7]), "r"(b.l[0]), "r"(b.l[1]), "r"(b.l[2]), "r"(b.l[3]), "r"(b.l[4]), "r"(b.l[5]),
+          "r"(b.l[6]), "r"(b.l[7]));
+    Fe<F> r;
+    // add N back when the subtraction borrowed (bw = 0xffffffff)
+    asm("add.cc.u32  %0, %8, %16;\n\t"
+        "addc.cc.u32 %1, %9, %17;\n\t"
+        "addc.cc.u32 %2, %10, %18;\n\t"
+        "addc.cc.u32 %3, %11, %19;\n\t"
+        "addc.cc.u32 %4, %12, %20;\n\t"
+        "addc.cc.u32 %5, %13, %21;\n\t"
+        "addc.cc.u32 %6, %14, %22;\n\t"
+        "addc.u32    %7, %15, %23;"
+        : "=r"(r.l[0]), "=r"(r.l[1]), "=r"(r.l[2]), "=r"(r.l[3]), "=r"(r.l[4]), "=r"(r.l[5]), "=r"(r.l[6]),
+          "=r"(r.l[7])
+        : "r"(d[0]), "r"(d[1]), "r"(d[2]), "r"(d[3]), "r"(d[4]), "r"(d[5]), "r"(d[6]), "r"(d[7]),
+          "r"(F::M0 & bw), "r"(F::M1 & bw), "r"(F::M2 & bw), "r"(F::M3 & bw), "r"(F::M4 & bw),
+          "r"(F::M5 & bw), "r"(F::M6 & bw), "r"(F::M7 & bw));
+    return r;
+}
+
+template <class F>
+__device__ __forceinline__ Fe<F> fe_neg(const Fe<F> &a) {
+    return fe_sub<F>(fe_zero<F>(), a);
+}
+
+template <class F>
+__device__ __forceinline__ Fe<F> fe_dbl(const Fe<F> &a) {
+    return fe_add<F>(a, a);
+}
+
+// a^e for a plain exponent given as 8 little-endian limbs, 4-bit fixed window.
+template <class F>
+__device__ __noinline__ Fe<F> fe_pow(const Fe<F> &a, const u32 e[8]) {
+    Fe<F> tab[16];
+    tab[0] = fe_one<F>();
+    tab[1] = a;
+#pragma unroll 1
+    for (int i = 2; i < 16; i++) tab[i] = fe_mul<F>(tab[i - 1], a);
+    Fe<F> acc = fe_one<F>();
+#pragma unroll 1
+    for (int nib = 63; nib >= 0; nib--) {
+        acc = fe_sqr<F>(acc);
+        acc = fe_sqr<F>(acc);
+        acc = fe_sqr<F>(acc);
+        acc = fe_sqr<F>(acc);
+        u32 v = (e[nib / 8] >> (4 * (nib % 8))) & 15u;
+        // table index is data-dependent; select through a loop to stay in registers
+        Fe<F> sel = tab[0];
+#pragma unroll
+        for (int k = 1; k < 16; k++)
+            if (v == (u32)k) sel = tab[k];
+        acc = fe_mul<F>(acc, sel);
+    }
+    return acc;
+}
+
+// Fermat inversion a^(N-2); inverse of zero is zero.
+template <class F>
+__device__ __forceinline__ Fe<F> fe_inv(const Fe<F> &a) {
+    u32 e[8] = {F::M0 - 2u, F::M1, F::M2, F::M3, F::M4, F::M5, F::M6, F::M7};
+    return fe_pow<F>(a, e);
+}
+
+template <class F>
+__device__ __forceinline__ Fe<F> fe_load(const u32 *p) {
+    Fe<F> r;
+    const uint4 *q = reinterpret_cast<const uint4 *>(p);
+    uint4 lo = q[0], hi = q[1];
+    r.l[0] = lo.x; r.l[1] = lo.y; r.l[2] = lo.z; r.l[3] = lo.w;
+    r.l[4] = hi.x; r.l[5] = hi.y; r.l[6] = hi.z; r.l[7] = hi.w;
+    return r;
+}
+
+template <class F>
+__device__ __forceinline__ void fe_store(u32 *p, const Fe<F> &a) {
+    uint4 *q = reinterpret_cast<uint4 *>(p);
+    q[0] = make_uint4(a.l[0], a.l[1], a.l[2], a.l[3]);
+    q[1] = make_uint4(a.l[4], a.l[5], a.l[6], a.l[7]);
+}
+
+// ---------------------------------------------------------------- G1 (XYZZ)
+
+struct Affine {
+    Fq x, y;
+};
+
+struct Xyzz {
+    Fq x, y, zz, zzz;
+};
+
+__device__ __forceinline__ bool affine_is_identity(const Affine &a) { return fe_is_zero(a.y); }
+
+__device__ __forceinline__ Xyzz xyzz_identity() {
+    Xyzz r;
+    r.x = fe_zero<FqP>();
+    r.y = fe_zero<FqP>();
+    r.zz = fe_zero<FqP>();
+    r.zzz = fe_zero<FqP>();
+    return r;
+}
+
+__device__ __forceinline__ bool xyzz_is_identity(const Xyzz &p) { return fe_is_zero(p.zz); }
+
+__device__ __forceinline__ Xyzz xyzz_from_affine(const Affine &a) {
+    if (affine_is_identity(a)) return xyzz_identity();
+    Xyzz r;
+    r.x = a.x;
+    r.y = a.y;
+    r.zz = fe_one<FqP>();
+    r.zzz = r.zz;
+    return r;
+}
+
+__device__ __forceinline__ Affine affine_neg(const Affine &a) {
+    Affine r;
+    r.x = a.x;
+    r.y = fe_neg<FqP>(a.y);
+    return r;
+}
+
+__device__ __forceinline__ Xyzz xyzz_neg(const Xyzz &p) {
+    Xyzz r = p;
+    r.y = fe_neg<FqP>(p.y);
+    return r;
+}
+
+// mdbl-2008-s-1: 2*a for an affine, non-identity a.
+__device__ __forceinline__ Xyzz affine_dbl(const Affine &a) {
+    Fq u = fe_dbl(a.y);
+    Fq v = fe_sqr(u);
+    Fq w = fe_mul(u, v);
+    Fq s = fe_mul(a.x, v);
+    Fq x2 = fe_sqr(a.x);
+    Fq m = fe_add(fe_dbl(x2), x2);
+    Xyzz r;
+    r.x = fe_sub(fe_sub(fe_sqr(m), s), s);
+    r.y = fe_sub(fe_mul(m, fe_sub(s, r.x)), fe_mul(w, a.y));
+    r.zz = v;
+    r.zzz = w;
+    return r;
+}
+
+// dbl-2008-s-1 with a = 0.
+__device__ __forceinline__ Xyzz xyzz_dbl(const Xyzz &p) {
+    if (xyzz_is_identity(p)) return p;
+    Fq u = fe_dbl(p.y);
+    Fq v = fe_sqr(u);
+    Fq w = fe_mul(u, v);
+    Fq s = fe_mul(p.x, v);
+    Fq x2 = fe_sqr(p.x);
+    Fq m = fe_add(fe_dbl(x2), x2);
+    Xyzz r;
+    r.x = fe_sub(fe_sub(fe_sqr(m), s), s);
+    r.y = fe_sub(fe_mul(m, fe_sub(s, r.x)), fe_mul(w, p.y));
+    r.zz = fe_mul(v, p.zz);
+    r.zzz = fe_mul(w, p.zzz);
+    return r;
+}
+
+// madd-2008-s: p + q, q affine.  Handles every special case.
+__device__ __forceinline__ Xyzz xyzz_add_affine(const Xyzz &p, const Affine &q) {
+    if (affine_is_identity(q)) return p;
+    if (xyzz_is_identity(p)) return xyzz_from_affine(q);
+    Fq u2 = fe_mul(q.x, p.zz);
+    Fq s2 = fe_mul(q.y, p.zzz);
+    Fq P = fe_sub(u2, p.x);
+    Fq R = fe_sub(s2, p.y);
+    if (fe_is_zero(P)) {
+        if (fe_is_zero(R)) return affine_dbl(q);
+        return xyzz_identity();
+    }
+    Fq pp = fe_sqr(P);
+    Fq ppp = fe_mul(P, pp);
+    Fq Q = fe_mul(p.x, pp);
+    Xyzz r;
+    r.zz = fe_mul(p.zz, pp);
+    r.zzz = fe_mul(p.zzz, ppp);
+    Fq t = fe_mul(p.y, ppp);
+    r.x = fe_sub(fe_sub(fe_sub(fe_sqr(R), ppp), Q), Q);
+    r.y = fe_sub(fe_mul(R, fe_sub(Q, r.x)), t);
+    return r;
+}
+
+// add-2008-s: p + q.  Handles every special case.
+__device__ __forceinline__ Xyzz xyzz_add(const Xyzz &p, const Xyzz &q) {
+    if (xyzz_is_identity(p)) return q;
+    if (xyzz_is_identity(q)) return p;
+    Fq u1 = fe_mul(p.x, q.zz);
+    Fq u2 = fe_mul(q.x, p.zz);
+    Fq s1 = fe_mul(p.y, q.zzz);
+    Fq s2 = fe_mul(q.y, p.zzz);
+    Fq P = fe_sub(u2, u1);
+    Fq R = fe_sub(s2, s1);
+    if (fe_is_zero(P)) {
+        if (fe_is_zero(R)) return xyzz_dbl(p);
+        return xyzz_identity();
+    }
+    Fq pp = fe_sqr(P);
+    Fq ppp = fe_mul(P, pp);
+    Fq Q = fe_mul(u1, pp);
+    Xyzz r;
+    r.zz = fe_mul(fe_mul(p.zz, q.zz), pp);
+    r.zzz = fe_mul(fe_mul(p.zzz, q.zzz), ppp);
+    Fq t = fe_mul(s1, ppp);
+    r.x = fe_sub(fe_sub(fe_sub(fe_sqr(R), ppp), Q), Q);
+    r.y = fe_sub(fe_mul(R, fe_sub(Q, r.x)), t);
+    return r;
+}
+
+// Canonical affine form; identity -> (0, 0).
+__device__ __forceinline__ Affine xyzz_to_affine(const Xyzz &p) {
+    Affine r;
+    if (xyzz_is_identity(p)) {
+        r.x = fe_zero<FqP>();
+        r.y = fe_zero<FqP>();
+        return r;
+    }
+    Fq a = fe_inv(p.zzz);
+    Fq b = fe_sqr(fe_mul(p.zz, a));
+    r.x = fe_mul(p.x, b);
+    r.y = fe_mul(p.y, a);
+    return r;
+}
+
+__device__ __forceinline__ Affine affine_load(const u32 *p) {
+    Affine a;
+    const uint4 *q = reinterpret_cast<const uint4 *>(p);
+    uint4 v0 = q[0], v1 = q[1], v2 = q[2], v3 = q[3];
+    a.x.l[0] = v0.x; a.x.l[1] = v0.y; a.x.l[2] = v0.z; a.x.l[3] = v0.w;
+    a.x.l[4] = v1.x; a.x.l[5] = v1.y; a.x.l[6] = v1.z; a.x.l[7] = v1.w;
+    a.y.l[0] = v2.x; a.y.l[1] = v2.y; a.y.l[2] = v2.z; a.y.l[3] = v2.w;
+    a.y.l[4] = v3.x; a.y.l[5] = v3.y; a.y.l[6] = v3.z; a.y.l[7] = v3.w;
+    return a;
+}
+
+__device__ __forceinline__ void affine_store(u32 *p, const Affine &a) {
+    fe_store(p, a.x);
+    fe_store(p + 8, a.y);
+}
+
+__device__ __forceinline__ Xyzz xyzz_load(const u32 *p) {
+    Xyzz r;
+    r.x = fe_load<FqP>(p);
+    r.y = fe_load<FqP>(p + 8);
+    r.zz = fe_load<FqP>(p + 16);
+    r.zzz = fe_load<FqP>(p + 24);
+    return r;
+}
+
+__device__ __forceinline__ void xyzz_store(u32 *p, const Xyzz &a) {
+    fe_store(p, a.x);
+    fe_store(p + 8, a.y);
+    fe_store(p + 16, a.zz);
+    fe_store(p + 24, a.zzz);
+}
+
+__device__ __forceinline__ Xyzz xyzz_shfl_down(const Xyzz &p, u32 delta, u32 mask = 0xffffffffu) {
+    Xyzz r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        r.x.l[i] = __shfl_down_sync(mask, p.x.l[i], delta);
+        r.y.l[i] = __shfl_down_sync(mask, p.y.l[i], delta);
+        r.zz.l[i] = __shfl_down_sync(mask, p.zz.l[i], delta);
+        r.zzz.l[i] = __shfl_down_sync(mask, p.zzz.l[i], delta);
+    }
+    return r;
+}
+
+// k * p for a small plain scalar k, left-to-right double-and-add.
+__device__ __forceinline__ Xyzz xyzz_mul_u32(const Xyzz &p, u32 k) {
+    Xyzz acc = xyzz_identity();
+    if (k == 0) return acc;
+    int top = 31 - __clz(k);
+#pragma unroll 1
+    for (int i = top; i >= 0; i--) {
+        acc = xyzz_dbl(acc);
+        if ((k >> i) & 1u) acc = xyzz_add(acc, p);
+    }
+    return acc;
+}
+
+}  // namespace bn254

@@ -1,0 +1,697 @@
+// MSM engine: plan layout, launch sequence, resident-SRS contexts, batches.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/impeller_msm.h"
+#include "engine.h"
+#include "msm_kernels.cuh"
+
+namespace impeller {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+const char *last_error() { return g_err.c_str(); }
+
+#define CK(x)                                                                                   \
+    do {                                                                                        \
+        cudaError_t _e = (x);                                                                   \
+        if (_e != cudaSuccess) {                                                                \
+            set_error(std::string(#x) + " failed: " + cudaGetErrorString(_e));                  \
+            return _e;                                                                          \
+        }                                                                                       \
+    } while (0)
+
+#define CK_LAUNCH(name)                                                                         \
+    do {                                                                                        \
+        cudaError_t _e = cudaGetLastError();                                                    \
+        if (_e != cudaSuccess) {                                                                \
+            set_error(std::string("launch of " name " failed: ") + cudaGetErrorString(_e));     \
+            return _e;                                                                          \
+        }                                                                                       \
+    } while (0)
+
+u32 digit_windows(u32 c) { return (254u + c - 1u) / c; }
+
+int sm_count(int device) {
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache.find(device);
+    if (it != cache.end()) return it->second;
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0) v = 148;
+    cache[device] = v;
+    return v;
+}
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
+    p.device = device;
+    p.shapes = shapes;
+    p.M = (u32)shapes.size();
+    if (p.M == 0) {
+        set_error("plan with no MSMs");
+        return false;
+    }
+    const int sms = sm_count(device);
+    std::vector<MsmDesc> descs(p.M);
+    std::vector<WinDesc> wins;
+    u64 nb = 0, entries = 0;
+    u32 nmax = 0;
+    for (u32 m = 0; m < p.M; m++) {
+        const MsmShape &s = shapes[m];
+        if (s.c < 3 || s.c > 31) {
+            set_error("window size must be in [3, 31]");
+            return false;
+        }
+        const u32 W = digit_windows(s.c);
+        const u32 nw = (s.n_windows == 0 || s.n_windows > W) ? W : s.n_windows;
+        const u32 n_tables = (W + nw - 1) / nw;
+        const u64 B = 1ull << (s.c - 1);
+        const u64 vmax = (u64)(n_tables - 1) * s.table_stride + s.n;
+        if (n_tables > 1 && s.table_stride < s.n) {
+            set_error("table stride smaller than the MSM size");
+            return false;
+        }
+        if (vmax >= (1ull << 31)) {
+            set_error("point index space (tables x length) exceeds 2^31");
+            return false;
+        }
+        MsmDesc &d = descs[m];
+        d.scalars = nullptr;
+        d.n = s.n;
+        d.c = s.c;
+        d.n_logical = W;
+        d.n_windows = nw;
+        d.table_stride = s.table_stride;
+        d.bucket_base = (u32)nb;
+        d.win_base = (u32)wins.size();
+        d.pad = 0;
+        for (u32 pw = 0; pw < nw; pw++) {
+            WinDesc w{};
+            w.bucket_base = (u32)(nb + pw * B);
+            w.nbuckets = (u32)B;
+            w.msm = m;
+            wins.push_back(w);
+        }
+        nb += nw * B;
+        entries += (u64)s.n * W;
+        nmax = std::max(nmax, s.n);
+        if (nb >= (1ull << 31) || entries >= 0xffffffffull) {
+            set_error("batch too large: bucket or entry count exceeds 32-bit indexing");
+            return false;
+        }
+    }
+    p.nb = (u32)nb;
+    p.nb_pad = (u32)align_up(nb, SCAN_TILE);
+    p.ntiles = p.nb_pad / SCAN_TILE;
+    p.max_entries = entries;
+
+    // reduce: chunk length per thread, partial-sum slots per window
+    const u64 target = (u64)sms * 512;
+    u32 L = 8;
+    while (nb / L > target && L < (1u << 30)) L <<= 1;
+    std::vector<uint2> rblocks;
+    u32 nparts = 0;
+    for (u32 wi = 0; wi < wins.size(); wi++) {
+        WinDesc &w = wins[wi];
+        w.chunk = std::min(L, w.nbuckets);
+        const u32 nthreads = (w.nbuckets + w.chunk - 1) / w.chunk;
+        const u32 nblocks = (nthreads + REDUCE_BLOCK - 1) / REDUCE_BLOCK;
+        w.part_base = nparts;
+        w.nparts = nblocks;
+        for (u32 k = 0; k < nblocks; k++) rblocks.push_back(make_uint2(wi, k));
+        nparts += nblocks;
+    }
+    p.nparts = nparts;
+    p.nwins = (u32)wins.size();
+    p.nrblocks = (u32)rblocks.size();
+
+    // accumulate: persistent threads, at least 8 entries each
+    const u32 full_blocks = (u32)sms * 2;
+    const u64 want_threads = (entries + 7) / 8;
+    p.accum_blocks = (u32)std::max<u64>(1, std::min<u64>(full_blocks, (want_threads + 255) / 256));
+    p.accum_block = 256;
+    const u32 T = p.accum_blocks * p.accum_block;
+    p.long_cap = T;
+    p.hist_grid_x = (u32)std::max<u64>(1, std::min<u64>((u64)sms * 8, (nmax + 255) / 256));
+
+    // host image of the tables
+    p.desc_off = 0;
+    p.win_off = align_up(sizeof(MsmDesc) * p.M, 16);
+    p.blk_off = p.win_off + align_up(sizeof(WinDesc) * wins.size(), 16);
+    const size_t tbytes = align_up(p.blk_off + sizeof(uint2) * rblocks.size(), 256);
+    p.tables.assign(tbytes, 0);
+    std::memcpy(p.tables.data() + p.desc_off, descs.data(), sizeof(MsmDesc) * p.M);
+    std::memcpy(p.tables.data() + p.win_off, wins.data(), sizeof(WinDesc) * wins.size());
+    std::memcpy(p.tables.data() + p.blk_off, rblocks.data(), sizeof(uint2) * rblocks.size());
+
+    // device scratch layout
+    PlanLayout &lo = p.layout;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    lo.o_tables = take(tbytes);
+    lo.tables_bytes = tbytes;
+    lo.o_counts = take((size_t)p.nb_pad * 4);
+    lo.o_cursor = take((size_t)p.nb * 4);
+    lo.o_offsets = take((size_t)(p.nb + 1) * 4);
+    lo.o_tiles = take((size_t)(p.ntiles + 1) * 4);
+    lo.o_entries = take((size_t)std::max<u64>(entries, 1) * 4);
+    lo.o_buckets = take((size_t)p.nb * 128);
+    lo.o_recb = take((size_t)2 * T * 4);
+    lo.o_recp = take((size_t)2 * T * 128);
+    lo.o_parts = take((size_t)nparts * 128);
+    lo.o_long = take((size_t)(1 + p.long_cap) * 4);
+    lo.o_carry = take((size_t)p.M * 128);
+    lo.o_results = take((size_t)p.M * 64);
+    lo.bytes = off;
+    return true;
+}
+
+Plan::~Plan() {
+    if (staging) cudaFreeHost(staging);
+    if (staged) cudaEventDestroy(staged);
+    for (auto &set : prof_sets)
+        for (auto e : set) cudaEventDestroy(e);
+}
+
+u32 Plan::launches() const { return 10; }
+
+const char *Plan::phase_name(int i) {
+    static const char *names[NPHASE] = {"tables", "histogram", "scan", "scatter",
+                                        "accumulate", "fixup", "reduce", "final"};
+    return (i >= 0 && i < NPHASE) ? names[i] : "";
+}
+
+cudaError_t Plan::prof_mark(int k, cudaStream_t st) {
+    if (!profiling) return cudaSuccess;
+    if (k == 0) {
+        if (prof_used == prof_sets.size()) {
+            std::vector<cudaEvent_t> set(NPHASE + 1);
+            for (auto &e : set) CK(cudaEventCreate(&e));
+            prof_sets.push_back(set);
+        }
+        prof_used++;
+    }
+    CK(cudaEventRecord(prof_sets[prof_used - 1][k], st));
+    return cudaSuccess;
+}
+
+cudaError_t Plan::read_profile(double *ms, u32 *runs) {
+    for (int i = 0; i < NPHASE; i++) ms[i] = 0;
+    for (u32 r = 0; r < prof_used; r++) {
+        CK(cudaEventSynchronize(prof_sets[r][NPHASE]));
+        for (int i = 0; i < NPHASE; i++) {
+            float t = 0;
+            CK(cudaEventElapsedTime(&t, prof_sets[r][i], prof_sets[r][i + 1]));
+            ms[i] += t;
+        }
+    }
+    if (runs) *runs = prof_used;
+    prof_used = 0;
+    return cudaSuccess;
+}
+
+cudaError_t Plan::stage(const u32 *const *scalars) {
+    if (!staging) {
+        CK(cudaSetDevice(device));
+        CK(cudaHostAlloc(&staging, tables.size(), cudaHostAllocPortable));
+        CK(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+    } else {
+        // the previous run's copy of the staging buffer must have finished
+        CK(cudaEventSynchronize(staged));
+    }
+    std::memcpy(staging, tables.data(), tables.size());
+    MsmDesc *d = reinterpret_cast<MsmDesc *>(static_cast<unsigned char *>(staging) + desc_off);
+    for (u32 m = 0; m < M; m++) d[m].scalars = scalars[m];
+    return cudaSuccess;
+}
+
+cudaError_t Plan::mark_staged(cudaStream_t st) {
+    CK(cudaEventRecord(staged, st));
+    return cudaSuccess;
+}
+
+cudaError_t Plan::launch(void *scratch, const u32 *points, u32 *results, int carry_mode, cudaStream_t st,
+                         u32 *carry_ext, bool record_staged) {
+    unsigned char *s = static_cast<unsigned char *>(scratch);
+    const MsmDesc *d_desc = reinterpret_cast<const MsmDesc *>(s + layout.o_tables + desc_off);
+    const WinDesc *d_wins = reinterpret_cast<const WinDesc *>(s + layout.o_tables + win_off);
+    const uint2 *d_blk = reinterpret_cast<const uint2 *>(s + layout.o_tables + blk_off);
+    u32 *counts = reinterpret_cast<u32 *>(s + layout.o_counts);
+    u32 *cursor = reinterpret_cast<u32 *>(s + layout.o_cursor);
+    u32 *offsets = reinterpret_cast<u32 *>(s + layout.o_offsets);
+    u32 *tiles = reinterpret_cast<u32 *>(s + layout.o_tiles);
+    u32 *entries = reinterpret_cast<u32 *>(s + layout.o_entries);
+    u32 *buckets = reinterpret_cast<u32 *>(s + layout.o_buckets);
+    u32 *recb = reinterpret_cast<u32 *>(s + layout.o_recb);
+    u32 *recp = reinterpret_cast<u32 *>(s + layout.o_recp);
+    u32 *parts = reinterpret_cast<u32 *>(s + layout.o_parts);
+    u32 *longl = reinterpret_cast<u32 *>(s + layout.o_long);
+    u32 *carry = carry_ext ? carry_ext : reinterpret_cast<u32 *>(s + layout.o_carry);
+    u32 *res = results ? results : reinterpret_cast<u32 *>(s + layout.o_results);
+
+    cudaError_t pe;
+#define MARK(k)                                  \
+    if ((pe = prof_mark((k), st)) != cudaSuccess) \
+        return pe;
+    MARK(0);
+    CK(cudaMemcpyAsync(s + layout.o_tables, staging, tables.size(), cudaMemcpyHostToDevice, st));
+    if (record_staged) CK(cudaEventRecord(staged, st));
+    CK(cudaMemsetAsync(counts, 0, (size_t)nb_pad * 4, st));
+    MARK(1);
+
+    dim3 hgrid(hist_grid_x, M);
+    k_histogram<<<hgrid, 256, 0, st>>>(d_desc, counts);
+    CK_LAUNCH("k_histogram");
+    MARK(2);
+    k_scan_reduce<<<ntiles, SCAN_BLOCK, 0, st>>>(counts, tiles);
+    CK_LAUNCH("k_scan_reduce");
+    k_scan_tiles<<<1, SCAN_BLOCK, 0, st>>>(tiles, ntiles);
+    CK_LAUNCH("k_scan_tiles");
+    k_scan_down<<<ntiles, SCAN_BLOCK, 0, st>>>(counts, tiles, offsets, cursor, nb, ntiles);
+    CK_LAUNCH("k_scan_down");
+    MARK(3);
+    k_scatter<<<hgrid, 256, 0, st>>>(d_desc, cursor, entries);
+    CK_LAUNCH("k_scatter");
+    MARK(4);
+
+    AccumArgs aa{entries, offsets, nb, points, buckets, recb, recp};
+    k_accumulate<<<accum_blocks, accum_block, 0, st>>>(aa);
+    CK_LAUNCH("k_accumulate");
+    MARK(5);
+
+    const u32 T = accum_blocks * accum_block;
+    CK(cudaMemsetAsync(longl, 0, 4, st));
+    FixupArgs fa{offsets, nb, T, recb, recp, buckets, longl, long_cap};
+    k_fixup_short<<<(T + 255) / 256, 256, 0, st>>>(fa);
+    CK_LAUNCH("k_fixup_short");
+    k_fixup_long<<<(u32)sm_count(device), 256, 0, st>>>(fa);
+    CK_LAUNCH("k_fixup_long");
+    MARK(6);
+
+    ReduceArgs ra{d_wins, d_blk, offsets, buckets, parts};
+    k_reduce<<<nrblocks, REDUCE_BLOCK, 0, st>>>(ra);
+    CK_LAUNCH("k_reduce");
+    MARK(7);
+
+    if (carry_mode == 0) {
+        FinalArgs fa2{d_desc, d_wins, parts, M, nullptr, 1, res};
+        k_final<<<(M + 31) / 32, 32, 0, st>>>(fa2);
+    } else {
+        FinalArgs fa2{d_desc, d_wins, parts, M, carry, carry_mode == 1 ? 1 : 0, res};
+        k_final<<<(M + 31) / 32, 32, 0, st>>>(fa2);
+    }
+    CK_LAUNCH("k_final");
+    MARK(8);
+#undef MARK
+    return cudaSuccess;
+}
+
+cudaError_t Plan::enqueue(void *scratch, const u32 *points, const u32 *const *scalars, u32 *results, int carry_mode,
+                          cudaStream_t stream, u32 *carry_ext) {
+    cudaError_t e = stage(scalars);
+    if (e != cudaSuccess) return e;
+    return launch(scratch, points, results, carry_mode, stream, carry_ext);
+}
+
+u32 *Plan::carry_ptr(void *scratch) const {
+    return reinterpret_cast<u32 *>(static_cast<unsigned char *>(scratch) + layout.o_carry);
+}
+
+u32 *Plan::results_ptr(void *scratch) const {
+    return reinterpret_cast<u32 *>(static_cast<unsigned char *>(scratch) + layout.o_results);
+}
+
+cudaError_t combine_xyzz(const u32 *d_xyzz, u32 k, u32 *d_out, cudaStream_t stream) {
+    k_combine<<<1, 32, 0, stream>>>(d_xyzz, k, d_out);
+    CK_LAUNCH("k_combine");
+    return cudaSuccess;
+}
+
+__global__ void k_precompute(u32 *points, u64 n, u32 shift, u32 n_tables) {
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Xyzz p = xyzz_from_affine(affine_load(points + i * 16));
+    for (u32 j = 1; j < n_tables; j++) {
+        for (u32 k = 0; k < shift; k++) p = xyzz_dbl(p);
+        affine_store(points + ((u64)j * n + i) * 16, xyzz_to_affine(p));
+    }
+}
+
+cudaError_t precompute_tables(u32 *d_points, u64 n, u32 shift, u32 n_tables, cudaStream_t stream) {
+    if (n == 0 || n_tables <= 1) return cudaSuccess;
+    k_precompute<<<(u32)((n + 127) / 128), 128, 0, stream>>>(d_points, n, shift, n_tables);
+    CK_LAUNCH("k_precompute");
+    return cudaSuccess;
+}
+
+// ------------------------------------------------------------ window table
+
+static std::mutex g_tab_mu;
+static std::vector<std::pair<u32, u32>> g_window_table;  // (log2 n, c)
+
+// Cost model used when no measured table is loaded: W(c) windows of n
+// mixed additions (10 Fq products each) plus the bucket reduction of
+// W(c) * 2^(c-1) buckets (two full additions, about 45 products with the
+// per-thread overhead of the chunked running sum).
+static u32 model_window(u64 n) {
+    u32 best = 8;
+    double best_cost = 1e300;
+    for (u32 c = 4; c <= 22; c++) {
+        double W = digit_windows(c);
+        double cost = W * ((double)n * 10.0 + std::ldexp(1.0, (int)c - 1) * 45.0);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
+
+u32 default_window(u64 n) {
+    if (n == 0) return 0;
+    std::lock_guard<std::mutex> g(g_tab_mu);
+    if (g_window_table.empty()) return model_window(n);
+    const double lg = std::log2((double)n);
+    u32 best = g_window_table[0].second;
+    double bd = 1e300;
+    for (auto &e : g_window_table) {
+        double dd = std::fabs(lg - (double)e.first);
+        if (dd < bd) {
+            bd = dd;
+            best = e.second;
+        }
+    }
+    return best;
+}
+
+}  // namespace impeller
+
+using namespace impeller;
+
+// -------------------------------------------------------------- contexts
+
+struct impeller_ctx {
+    int device = 0;
+    const u32 *points = nullptr;
+    u64 len = 0;
+    bool owns = false;
+    std::mutex mu;
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    u32 *d_scalars = nullptr;  // staging for impeller_msm_host
+    u64 d_scalars_cap = 0;
+    u32 *d_result = nullptr;
+    cudaEvent_t done = nullptr;  // last run that used the scratch
+    bool profiling = false;
+    std::map<std::pair<u32, u32>, std::unique_ptr<Plan>> plans;
+};
+
+static cudaError_t ctx_reserve(impeller_ctx *ctx, size_t bytes, cudaStream_t st) {
+    if (bytes <= ctx->scratch_bytes) return cudaSuccess;
+    CK(cudaStreamSynchronize(st));
+    CK(cudaEventSynchronize(ctx->done));
+    if (ctx->scratch) CK(cudaFree(ctx->scratch));
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    CK(cudaMalloc(&ctx->scratch, bytes));
+    ctx->scratch_bytes = bytes;
+    return cudaSuccess;
+}
+
+static Plan *ctx_plan(impeller_ctx *ctx, u32 n, u32 c) {
+    auto key = std::make_pair(n, c);
+    auto it = ctx->plans.find(key);
+    if (it != ctx->plans.end()) return it->second.get();
+    std::unique_ptr<Plan> p(new Plan());
+    if (!Plan::build(*p, ctx->device, {MsmShape{n, c, 0, 0}})) return nullptr;
+    Plan *raw = p.get();
+    raw->set_profiling(ctx->profiling);
+    ctx->plans[key] = std::move(p);
+    return raw;
+}
+
+extern "C" {
+
+const char *impeller_last_error(void) { return impeller::last_error(); }
+
+const char *impeller_version(void) { return "impeller-b200-msm 0.1 (sm_100a)"; }
+
+unsigned int impeller_default_window(uint64_t n) { return impeller::default_window(n); }
+
+cudaError_t impeller_set_window_table(const uint32_t *log2n, const uint32_t *c, uint32_t count) {
+    std::vector<std::pair<u32, u32>> t;
+    for (u32 i = 0; i < count; i++) {
+        if (c[i] < 3 || c[i] > 31) {
+            set_error("window table entry outside [3, 31]");
+            return cudaErrorInvalidValue;
+        }
+        t.emplace_back(log2n[i], c[i]);
+    }
+    std::lock_guard<std::mutex> g(g_tab_mu);
+    g_window_table = t;
+    return cudaSuccess;
+}
+
+cudaError_t impeller_ctx_create(impeller_ctx **out, int device, const uint32_t *points, uint64_t len,
+                                int points_on_device) {
+    if (!out || (!points && len)) {
+        set_error("impeller_ctx_create: null argument");
+        return cudaErrorInvalidValue;
+    }
+    if (len >= (1ull << 31)) {
+        set_error("impeller_ctx_create: at most 2^31 - 1 points");
+        return cudaErrorInvalidValue;
+    }
+    std::unique_ptr<impeller_ctx> ctx(new impeller_ctx());
+    ctx->device = device;
+    ctx->len = len;
+    CK(cudaSetDevice(device));
+    CK(cudaEventCreateWithFlags(&ctx->done, cudaEventDisableTiming));
+    if (points_on_device) {
+        ctx->points = points;
+    } else {
+        u32 *d = nullptr;
+        CK(cudaMalloc(&d, std::max<u64>(len, 1) * 64));
+        cudaError_t e = cudaMemcpy(d, points, len * 64, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(d);
+            set_error(std::string("impeller_ctx_create: upload failed: ") + cudaGetErrorString(e));
+            return e;
+        }
+        ctx->points = d;
+        ctx->owns = true;
+    }
+    CK(cudaMalloc(&ctx->d_result, 64));
+    *out = ctx.release();
+    return cudaSuccess;
+}
+
+cudaError_t impeller_ctx_destroy(impeller_ctx *ctx) {
+    if (!ctx) return cudaSuccess;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    if (ctx->owns) cudaFree(const_cast<u32 *>(ctx->points));
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->d_scalars) cudaFree(ctx->d_scalars);
+    if (ctx->d_result) cudaFree(ctx->d_result);
+    if (ctx->done) cudaEventDestroy(ctx->done);
+    ctx->plans.clear();
+    delete ctx;
+    return cudaSuccess;
+}
+
+const uint32_t *impeller_ctx_points(const impeller_ctx *ctx) { return ctx ? ctx->points : nullptr; }
+uint64_t impeller_ctx_len(const impeller_ctx *ctx) { return ctx ? ctx->len : 0; }
+
+static cudaError_t ctx_run_locked(impeller_ctx *ctx, const uint32_t *d_scalars, uint64_t n, unsigned int c,
+                                  uint32_t *d_result, cudaStream_t stream) {
+    if (n > ctx->len) {
+        set_error("MSM larger than the resident point array");
+        return cudaErrorInvalidValue;
+    }
+    if (n == 0) return cudaMemsetAsync(d_result, 0, 64, stream);
+    if (c == 0) c = default_window(n);
+    CK(cudaSetDevice(ctx->device));
+    Plan *p = ctx_plan(ctx, (u32)n, c);
+    if (!p) return cudaErrorInvalidValue;
+    cudaError_t e = ctx_reserve(ctx, p->scratch_bytes(), stream);
+    if (e != cudaSuccess) return e;
+    CK(cudaStreamWaitEvent(stream, ctx->done, 0));
+    const u32 *sc[1] = {d_scalars};
+    e = p->enqueue(ctx->scratch, ctx->points, sc, d_result, 0, stream);
+    if (e != cudaSuccess) return e;
+    CK(cudaEventRecord(ctx->done, stream));
+    return cudaSuccess;
+}
+
+cudaError_t impeller_msm_device(impeller_ctx *ctx, const uint32_t *d_scalars, uint64_t n, unsigned int c,
+                                uint32_t *d_result, cudaStream_t stream) {
+    if (!ctx || (!d_scalars && n) || !d_result) {
+        set_error("impeller_msm_device: null argument");
+        return cudaErrorInvalidValue;
+    }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    return ctx_run_locked(ctx, d_scalars, n, c, d_result, stream);
+}
+
+cudaError_t impeller_msm_host(impeller_ctx *ctx, const uint32_t *h_scalars, uint64_t n, unsigned int c,
+                              uint32_t *h_result, cudaStream_t stream) {
+    if (!ctx || (!h_scalars && n) || !h_result) {
+        set_error("impeller_msm_host: null argument");
+        return cudaErrorInvalidValue;
+    }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    CK(cudaSetDevice(ctx->device));
+    if (n > ctx->d_scalars_cap) {
+        CK(cudaStreamSynchronize(stream));
+        CK(cudaEventSynchronize(ctx->done));
+        if (ctx->d_scalars) CK(cudaFree(ctx->d_scalars));
+        ctx->d_scalars = nullptr;
+        ctx->d_scalars_cap = 0;
+        CK(cudaMalloc(&ctx->d_scalars, n * 32));
+        ctx->d_scalars_cap = n;
+    }
+    // the previous run read d_scalars: order the copy after it
+    CK(cudaStreamWaitEvent(stream, ctx->done, 0));
+    if (n) CK(cudaMemcpyAsync(ctx->d_scalars, h_scalars, n * 32, cudaMemcpyHostToDevice, stream));
+    cudaError_t e = ctx_run_locked(ctx, ctx->d_scalars, n, c, ctx->d_result, stream);
+    if (e != cudaSuccess) return e;
+    CK(cudaMemcpyAsync(h_result, ctx->d_result, 64, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return cudaSuccess;
+}
+
+cudaError_t impeller_ctx_profile(impeller_ctx *ctx, int enable) {
+    if (!ctx) return cudaErrorInvalidValue;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->profiling = enable != 0;
+    for (auto &kv : ctx->plans) kv.second->set_profiling(ctx->profiling);
+    return cudaSuccess;
+}
+
+cudaError_t impeller_ctx_profile_read(impeller_ctx *ctx, double *ms_per_phase, uint32_t nphase, uint32_t *runs) {
+    if (!ctx || !ms_per_phase || nphase < (u32)Plan::NPHASE) {
+        set_error("impeller_ctx_profile_read: need room for every phase");
+        return cudaErrorInvalidValue;
+    }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    for (u32 i = 0; i < nphase; i++) ms_per_phase[i] = 0;
+    u32 total = 0;
+    for (auto &kv : ctx->plans) {
+        double ms[Plan::NPHASE];
+        u32 r = 0;
+        cudaError_t e = kv.second->read_profile(ms, &r);
+        if (e != cudaSuccess) return e;
+        for (int i = 0; i < Plan::NPHASE; i++) ms_per_phase[i] += ms[i];
+        total += r;
+    }
+    if (runs) *runs = total;
+    return cudaSuccess;
+}
+
+const char *impeller_phase_name(uint32_t i) { return Plan::phase_name((int)i); }
+
+// ---------------------------------------------------------------- batches
+
+}  // extern "C"
+
+struct impeller_batch {
+    impeller_ctx *ctx = nullptr;
+    Plan plan;
+    void *scratch = nullptr;
+    bool graph = false;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cap_stream = nullptr;
+};
+
+extern "C" {
+
+cudaError_t impeller_batch_create(impeller_batch **out, impeller_ctx *ctx, const uint64_t *sizes,
+                                  const unsigned int *windows, uint32_t count, uint32_t flags) {
+    if (!out || !ctx || !sizes || count == 0) {
+        set_error("impeller_batch_create: bad argument");
+        return cudaErrorInvalidValue;
+    }
+    std::vector<MsmShape> shapes;
+    for (u32 i = 0; i < count; i++) {
+        if (sizes[i] > ctx->len || sizes[i] == 0) {
+            set_error("impeller_batch_create: size 0 or larger than the resident point array");
+            return cudaErrorInvalidValue;
+        }
+        u32 c = windows && windows[i] ? windows[i] : default_window(sizes[i]);
+        shapes.push_back(MsmShape{(u32)sizes[i], c, 0, 0});
+    }
+    std::unique_ptr<impeller_batch> b(new impeller_batch());
+    b->ctx = ctx;
+    if (!Plan::build(b->plan, ctx->device, shapes)) return cudaErrorInvalidValue;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMalloc(&b->scratch, b->plan.scratch_bytes()));
+    b->graph = (flags & IMPELLER_BATCH_GRAPH) != 0;
+    *out = b.release();
+    return cudaSuccess;
+}
+
+cudaError_t impeller_batch_destroy(impeller_batch *b) {
+    if (!b) return cudaSuccess;
+    cudaSetDevice(b->ctx->device);
+    cudaDeviceSynchronize();
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->g) cudaGraphDestroy(b->g);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    if (b->scratch) cudaFree(b->scratch);
+    delete b;
+    return cudaSuccess;
+}
+
+uint32_t impeller_batch_launches(const impeller_batch *b) { return b ? b->plan.launches() : 0; }
+
+cudaError_t impeller_batch_run(impeller_batch *b, const uint32_t *const *d_scalars, uint32_t *d_results,
+                               cudaStream_t stream) {
+    if (!b || !d_scalars || !d_results) {
+        set_error("impeller_batch_run: null argument");
+        return cudaErrorInvalidValue;
+    }
+    CK(cudaSetDevice(b->ctx->device));
+    cudaError_t e = b->plan.stage(d_scalars);
+    if (e != cudaSuccess) return e;
+    if (!b->graph) {
+        e = b->plan.launch(b->scratch, b->ctx->points, nullptr, 0, stream);
+        if (e != cudaSuccess) return e;
+    } else {
+        if (!b->exec) {
+            CK(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+            CK(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+            e = b->plan.launch(b->scratch, b->ctx->points, nullptr, 0, b->cap_stream, nullptr, false);
+            cudaGraph_t g = nullptr;
+            cudaError_t e2 = cudaStreamEndCapture(b->cap_stream, &g);
+            if (e != cudaSuccess) return e;
+            CK(e2);
+            b->g = g;
+            CK(cudaGraphInstantiate(&b->exec, g, 0));
+        }
+        CK(cudaGraphLaunch(b->exec, stream));
+        e = b->plan.mark_staged(stream);
+        if (e != cudaSuccess) return e;
+    }
+    CK(cudaMemcpyAsync(d_results, b->plan.results_ptr(b->scratch), (size_t)b->plan.M * 64, cudaMemcpyDeviceToDevice,
+                       stream));
+    return cudaSuccess;
+}
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+// Host-side MSM engine: plans a batch of MSMs over one device point array,
+// lays out its device scratch, and enqueues the kernel sequence on a stream.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace impeller {
+
+typedef uint32_t u32;
+typedef uint64_t u64;
+
+void set_error(const std::string &msg);
+const char *last_error();
+
+// Shape of one MSM in a plan.
+struct MsmShape {
+    u32 n;             // points / scalars
+    u32 c;             // window bits
+    u32 n_windows;     // bucket sets (physical windows); 0 -> one per digit window
+    u32 table_stride;  // points per window table (used when n_windows < digit windows)
+};
+
+u32 digit_windows(u32 c);  // ceil(254 / c)
+u32 default_window(u64 n);  // autotune table (or the cost model)
+
+// Device property cache.
+int sm_count(int device);
+
+struct PlanLayout {
+    size_t o_tables, tables_bytes;  // descs | wins | reduce blocks (uploaded each run)
+    size_t o_counts, o_cursor, o_offsets, o_tiles, o_entries, o_buckets;
+    size_t o_recb, o_recp, o_parts, o_long, o_carry, o_results;
+    size_t bytes;
+};
+
+class Plan {
+  public:
+    // Every MSM reads points[(w / n_windows) * table_stride + i].
+    static bool build(Plan &p, int device, const std::vector<MsmShape> &shapes);
+    ~Plan();
+
+    // Enqueue one run.  scalars[m] are device pointers.  carry_mode:
+    // 0 = plain (results are affine), 1 = add the XYZZ carry in and emit
+    // affine, 2 = add the carry in and keep XYZZ in the carry (no affine).
+    // results may be null (results stay in scratch at layout.o_results).
+    // carry_ext, when given, replaces the plan's own carry slots (M XYZZ).
+    cudaError_t enqueue(void *scratch, const u32 *points, const u32 *const *scalars, u32 *results, int carry_mode,
+                        cudaStream_t stream, u32 *carry_ext = nullptr);
+    // enqueue == stage (host: write the pinned table image with these scalar
+    // pointers, after the previous run's copy of it finished) + launch
+    // (stream: copy the image, run the kernels).  launch alone is what a
+    // CUDA graph captures; stage before every replay.
+    cudaError_t stage(const u32 *const *scalars);
+    // record_staged = false while capturing a CUDA graph: an event recorded
+    // inside a capture cannot be waited on from the host, so the graph's
+    // caller marks the staging buffer free after the graph launch instead.
+    cudaError_t launch(void *scratch, const u32 *points, u32 *results, int carry_mode, cudaStream_t stream,
+                       u32 *carry_ext = nullptr, bool record_staged = true);
+    cudaError_t mark_staged(cudaStream_t stream);
+
+    size_t scratch_bytes() const { return layout.bytes; }
+    u32 launches() const;
+    u32 *carry_ptr(void *scratch) const;
+    u32 *results_ptr(void *scratch) const;
+
+    int device = 0;
+    u32 M = 0;
+    u32 nb = 0, nb_pad = 0, ntiles = 0;
+    u64 max_entries = 0;
+    u32 accum_blocks = 0, accum_block = 256;
+    u32 nparts = 0, long_cap = 0;
+    u32 hist_grid_x = 1;
+    std::vector<MsmShape> shapes;
+    PlanLayout layout{};
+
+    // Per-phase timing: when enabled, every launch records CUDA events on the
+    // launching stream between phases; read_profile sums the recorded runs.
+    static constexpr int NPHASE = 8;
+    static const char *phase_name(int i);
+    void set_profiling(bool on) { profiling = on; }
+    cudaError_t read_profile(double *ms_per_phase, u32 *runs);
+
+    Plan() = default;
+    Plan(const Plan &) = delete;
+    Plan &operator=(const Plan &) = delete;
+
+  private:
+    void *staging = nullptr;     // pinned copy of the tables
+    cudaEvent_t staged = nullptr;
+    std::vector<unsigned char> tables;  // host image of the tables
+    size_t desc_off = 0, win_off = 0, blk_off = 0;
+    u32 nwins = 0, nrblocks = 0;
+    bool profiling = false;
+    std::vector<std::vector<cudaEvent_t>> prof_sets;  // one set of NPHASE+1 events per run
+    u32 prof_used = 0;
+    cudaError_t prof_mark(int k, cudaStream_t st);
+};
+
+// k_combine: sum `k` XYZZ points in device memory, write canonical affine.
+cudaError_t combine_xyzz(const u32 *d_xyzz, u32 k, u32 *d_out, cudaStream_t stream);
+
+// Window tables 2^(j*shift)*P for j in 1..n_tables-1, in place after table 0.
+cudaError_t precompute_tables(u32 *d_points, u64 n, u32 shift, u32 n_tables, cudaStream_t stream);
+
+}  // namespace impeller

@@ -1,0 +1,436 @@
+// Pippenger MSM kernels for BN254 G1 on sm_100a.
+//
+// One pass over a batch of M MSMs that share one device-resident point array:
+//
+//   k_histogram   scalar (Montgomery Fr) -> canonical -> signed c-bit digits;
+//                 count entries per bucket                      [HBM-bound]
+//   k_scan_*      exclusive scan of the bucket counts -> bucket offsets
+//   k_scatter     same digits; place (point index, sign) of every nonzero
+//                 digit into its bucket's slice of `entries`     [HBM-bound]
+//   k_accumulate  persistent threads walk equal slices of `entries`, one
+//                 XYZZ += affine (madd-2008-s) per entry; buckets that fit in
+//                 one slice are written directly, buckets cut by a slice
+//                 boundary leave partial sums                  [IMAD-bound]
+//   k_fixup_*     merge the partial sums of cut buckets (short runs per
+//                 thread, long runs -- heavy buckets -- per warp)
+//   k_reduce      per window sum_k k * S_k by chunked running sums
+//   k_final       per MSM Horner combine of the windows, affine conversion
+//
+// Differences from the reference (core/src/msm/src/msm_impl.cuh): the
+// reference sorts 64-bit keys with CUB radix sort (:459-463), protects the
+// first bucket of each thread slice with a spin mutex (:73-105, :189-204),
+// finishes the sum of the reduce blocks and the affine conversion on the host
+// (:716-733, core/src/msm/src/msm.cu:37-39).  Here the sort is a counting
+// sort by bucket, cut buckets are merged without locks, and every step up to
+// the canonical affine result runs on the device.
+#pragma once
+
+#include "bn254.cuh"
+
+namespace impeller {
+
+using namespace bn254;
+
+static constexpr u32 NONE = 0xffffffffu;
+static constexpr u32 SCAN_BLOCK = 256;
+static constexpr u32 SCAN_PER_THREAD = 16;
+static constexpr u32 SCAN_TILE = SCAN_BLOCK * SCAN_PER_THREAD;
+
+// One MSM of a batch.  Virtual point index of digit window w of scalar i is
+// (w / n_windows) * table_stride + i: window tables hold 2^(j*n_windows*c)*P
+// (core/src/msm/src/msm.cuh:53-70 for the window / table relation).
+struct MsmDesc {
+    const u32 *scalars;  // n x 8 u32, Montgomery Fr
+    u32 n;
+    u32 c;               // window bits
+    u32 n_logical;       // ceil(254 / c) digit windows
+    u32 n_windows;       // bucket sets (physical windows)
+    u32 table_stride;    // points per window table
+    u32 bucket_base;     // global index of bucket (window 0, weight 1)
+    u32 win_base;        // global index of physical window 0
+    u32 pad;
+};
+
+// One physical window of one MSM (bucket reduction unit).
+struct WinDesc {
+    u32 bucket_base;  // global index of the weight-1 bucket of this window
+    u32 nbuckets;     // 2^(c-1)
+    u32 chunk;        // buckets per reduce thread
+    u32 part_base;    // first partial-sum slot of this window
+    u32 nparts;       // number of partial-sum slots (reduce blocks)
+    u32 msm;          // owning MSM
+    u32 pad0, pad1;
+};
+
+__device__ __forceinline__ u32 limb_at(const Fr &v, u32 idx) {
+    u32 r = 0;
+#pragma unroll
+    for (u32 k = 0; k < 8; k++)
+        if (k == idx) r = v.l[k];
+    return r;
+}
+
+// Signed-digit recoding of the reference (core/src/msm/src/msm_impl.cuh:22-33):
+// a digit >= 2^(c-1) becomes digit - 2^c and carries into the next window.
+// The top window is never recoded: for every 3 <= c <= 31, r < 2^254 keeps
+// the top digit plus an incoming carry at most 2^(c-1), a valid bucket.
+struct DigitIter {
+    Fr v;
+    u32 c, carry;
+    __device__ __forceinline__ void next(u32 w, u32 n_logical, u32 &mag, u32 &sign) {
+        u32 o = w * c;
+        u32 idx = o >> 5, sh = o & 31u;
+        u32 raw = __funnelshift_r(limb_at(v, idx), limb_at(v, idx + 1), sh) & ((1u << c) - 1u);
+        u32 d = raw + carry;
+        u32 half = 1u << (c - 1);
+        if (d >= half && w + 1 < n_logical) {
+            // d >= 2^(c-1) on a non-top window: negative digit d - 2^c
+            mag = (1u << c) - d;
+            sign = 1;
+            carry = 1;
+        } else {
+            mag = d;
+            sign = 0;
+            carry = 0;
+        }
+    }
+};
+
+__global__ void k_histogram(const MsmDesc *__restrict__ descs, u32 *__restrict__ counts) {
+    const MsmDesc d = descs[blockIdx.y];
+    const u32 B = 1u << (d.c - 1);
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
+        DigitIter it;
+        it.v = fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i));
+        it.c = d.c;
+        it.carry = 0;
+        for (u32 w = 0; w < d.n_logical; w++) {
+            u32 mag, sign;
+            it.next(w, d.n_logical, mag, sign);
+            if (mag) {
+                u32 pw = w % d.n_windows;
+                atomicAdd(&counts[d.bucket_base + pw * B + mag - 1], 1u);
+            }
+        }
+    }
+}
+
+__global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ cursor, u32 *__restrict__ entries) {
+    const MsmDesc d = descs[blockIdx.y];
+    const u32 B = 1u << (d.c - 1);
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
+        DigitIter it;
+        it.v = fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i));
+        it.c = d.c;
+        it.carry = 0;
+        for (u32 w = 0; w < d.n_logical; w++) {
+            u32 mag, sign;
+            it.next(w, d.n_logical, mag, sign);
+            if (mag) {
+                u32 pw = w % d.n_windows;
+                u32 table = w / d.n_windows;
+                u32 pos = atomicAdd(&cursor[d.bucket_base + pw * B + mag - 1], 1u);
+                entries[pos] = ((table * d.table_stride + i) << 1) | sign;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------- scan
+
+__device__ __forceinline__ u32 block_exclusive_scan(u32 v, u32 &total) {
+    __shared__ u32 warp_tot[SCAN_BLOCK / 32];
+    const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    u32 x = v;
+#pragma unroll
+    for (u32 o = 1; o < 32; o <<= 1) {
+        u32 y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        u32 t = lane < SCAN_BLOCK / 32 ? warp_tot[lane] : 0;
+#pragma unroll
+        for (u32 o = 1; o < 32; o <<= 1) {
+            u32 y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < SCAN_BLOCK / 32) warp_tot[lane] = t;
+    }
+    __syncthreads();
+    total = warp_tot[SCAN_BLOCK / 32 - 1];
+    u32 before = wid ? warp_tot[wid - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+// counts must be padded to a multiple of SCAN_TILE with zeros.
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_reduce(const u32 *__restrict__ counts, u32 *__restrict__ tile_sums) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(counts + (size_t)blockIdx.x * SCAN_TILE) + threadIdx.x * 4;
+    u32 s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        uint4 v = p[k];
+        s += v.x + v.y + v.z + v.w;
+    }
+    u32 total;
+    block_exclusive_scan(s, total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// Single block: exclusive scan of the tile sums in place; tile_sums[ntiles]
+// receives the grand total.
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_tiles(u32 *__restrict__ tile_sums, u32 ntiles) {
+    u32 carry = 0;
+    for (u32 base = 0; base < ntiles; base += SCAN_BLOCK) {
+        u32 i = base + threadIdx.x;
+        u32 v = i < ntiles ? tile_sums[i] : 0;
+        u32 total;
+        u32 ex = block_exclusive_scan(v, total);
+        if (i < ntiles) tile_sums[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) tile_sums[ntiles] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_down(const u32 *__restrict__ counts, const u32 *__restrict__ tile_sums,
+                                                   u32 *__restrict__ offsets, u32 *__restrict__ cursor, u32 nb,
+                                                   u32 ntiles) {
+    const size_t base = (size_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER_THREAD;
+    const uint4 *p = reinterpret_cast<const uint4 *>(counts + base);
+    u32 v[SCAN_PER_THREAD];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        uint4 q = p[k];
+        v[4 * k] = q.x; v[4 * k + 1] = q.y; v[4 * k + 2] = q.z; v[4 * k + 3] = q.w;
+    }
+    u32 s = 0;
+#pragma unroll
+    for (int k = 0; k < (int)SCAN_PER_THREAD; k++) s += v[k];
+    u32 total;
+    u32 run = block_exclusive_scan(s, total) + tile_sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < (int)SCAN_PER_THREAD; k++) {
+        size_t i = base + k;
+        if (i < nb) {
+            offsets[i] = run;
+            cursor[i] = run;
+        }
+        run += v[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) offsets[nb] = tile_sums[ntiles];
+}
+
+// ------------------------------------------------------------- accumulate
+
+struct AccumArgs {
+    const u32 *entries;
+    const u32 *offsets;  // nb + 1
+    u32 nb;
+    const u32 *points;   // affine, 16 u32 each
+    u32 *buckets;        // XYZZ, 32 u32 each, indexed by global bucket
+    u32 *rec_bucket;     // 2 per thread
+    u32 *rec_point;      // 2 per thread, XYZZ
+};
+
+__device__ __forceinline__ Affine load_entry_point(const u32 *__restrict__ points, u32 e) {
+    Affine q = affine_load(points + (size_t)(e >> 1) * 16);
+    if (e & 1u) q.y = fe_neg<FqP>(q.y);
+    return q;
+}
+
+// Thread t owns entries [t*L, min((t+1)*L, E)), L = ceil(E / T).
+// A bucket whose entries all fall in one slice is written to `buckets`.
+// Otherwise the slice leaves a record: slot 2t for a piece that continues a
+// bucket begun in an earlier slice, slot 2t+1 for a piece whose bucket begins
+// in this slice and continues in later ones.
+__global__ void __launch_bounds__(256, 2) k_accumulate(AccumArgs a) {
+    const u32 T = gridDim.x * blockDim.x;
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 E = a.offsets[a.nb];
+    const u32 L = (E + T - 1) / T;
+    const u64 start64 = (u64)t * L;
+    const u32 start = (u32)min(start64, (u64)E);
+    const u32 end = (u32)min(start64 + L, (u64)E);
+    a.rec_bucket[2 * t] = NONE;
+    a.rec_bucket[2 * t + 1] = NONE;
+    if (start >= end) return;
+
+    // largest b with offsets[b] <= start
+    u32 lo = 0, hi = a.nb;
+    while (hi - lo > 1) {
+        u32 mid = (lo + hi) >> 1;
+        if (a.offsets[mid] <= start) lo = mid;
+        else hi = mid;
+    }
+    u32 b = lo;
+    u32 bbeg = a.offsets[b], bend = a.offsets[b + 1];
+    u32 seg_end = min(bend, end);
+
+    Xyzz acc = xyzz_identity();
+    bool fresh = true;
+    Affine nxt = load_entry_point(a.points, a.entries[start]);
+    for (u32 pos = start; pos < end; pos++) {
+        Affine q = nxt;
+        if (pos + 1 < end) nxt = load_entry_point(a.points, a.entries[pos + 1]);
+        if (fresh) {
+            acc = xyzz_from_affine(q);
+            fresh = false;
+        } else {
+            acc = xyzz_add_affine(acc, q);
+        }
+        if (pos + 1 == seg_end) {
+            if (bbeg >= start && bend <= end) {
+                xyzz_store(a.buckets + (size_t)b * 32, acc);
+            } else {
+                u32 slot = bbeg < start ? 2 * t : 2 * t + 1;
+                a.rec_bucket[slot] = b;
+                xyzz_store(a.rec_point + (size_t)slot * 32, acc);
+            }
+            fresh = true;
+            if (pos + 1 < end) {
+                do {
+                    b++;
+                    bend = a.offsets[b + 1];
+                } while (bend <= pos + 1);
+                bbeg = a.offsets[b];
+                seg_end = min(bend, end);
+            }
+        }
+    }
+}
+
+struct FixupArgs {
+    const u32 *offsets;
+    u32 nb;
+    u32 T;               // accumulate threads
+    const u32 *rec_bucket;
+    const u32 *rec_point;
+    u32 *buckets;
+    u32 *long_list;      // [0] = count, then owner thread ids
+    u32 long_cap;
+};
+
+// Owner of a cut bucket = the slice where the bucket begins (record 2t+1).
+// The bucket continues as the first piece (record 2t') of slices t+1 .. t1.
+__global__ void k_fixup_short(FixupArgs f) {
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= f.T) return;
+    const u32 b = f.rec_bucket[2 * t + 1];
+    if (b == NONE) return;
+    const u32 E = f.offsets[f.nb];
+    const u32 L = (E + f.T - 1) / f.T;
+    const u32 t1 = (f.offsets[b + 1] - 1) / L;
+    if (t1 - t > 4) {
+        u32 k = atomicAdd(&f.long_list[0], 1u);
+        if (k < f.long_cap) f.long_list[1 + k] = t;
+        return;
+    }
+    Xyzz acc = xyzz_load(f.rec_point + (size_t)(2 * t + 1) * 32);
+    for (u32 s = t + 1; s <= t1; s++) acc = xyzz_add(acc, xyzz_load(f.rec_point + (size_t)(2 * s) * 32));
+    xyzz_store(f.buckets + (size_t)b * 32, acc);
+}
+
+// One warp per long run (a bucket spread over more than 5 slices).
+__global__ void k_fixup_long(FixupArgs f) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
+    const u32 count = min(f.long_list[0], f.long_cap);
+    const u32 E = f.offsets[f.nb];
+    const u32 L = (E + f.T - 1) / f.T;
+    for (u32 w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += nwarps) {
+        const u32 t = f.long_list[1 + w];
+        const u32 b = f.rec_bucket[2 * t + 1];
+        const u32 t1 = (f.offsets[b + 1] - 1) / L;
+        Xyzz acc = xyzz_identity();
+        if (lane == 0) acc = xyzz_load(f.rec_point + (size_t)(2 * t + 1) * 32);
+        for (u32 s = t + 1 + lane; s <= t1; s += 32) acc = xyzz_add(acc, xyzz_load(f.rec_point + (size_t)(2 * s) * 32));
+#pragma unroll 1
+        for (u32 o = 16; o; o >>= 1) acc = xyzz_add(acc, xyzz_shfl_down(acc, o));
+        if (lane == 0) xyzz_store(f.buckets + (size_t)b * 32, acc);
+    }
+}
+
+// ----------------------------------------------------------------- reduce
+
+struct ReduceArgs {
+    const WinDesc *wins;
+    const uint2 *blocks;  // (window, block-in-window) per reduce block
+    const u32 *offsets;
+    const u32 *buckets;
+    u32 *parts;           // XYZZ partial per reduce block
+};
+
+static constexpr u32 REDUCE_BLOCK = 128;
+
+// Thread j of window w sums the chunk of weights (j*L, (j+1)*L]:
+// running sums from the top give sum_k (k - j*L) * S_k and sum_k S_k;
+// adding (j*L) * sum_k S_k gives the chunk's share of sum_k k * S_k.
+__global__ void __launch_bounds__(REDUCE_BLOCK) k_reduce(ReduceArgs r) {
+    __shared__ __align__(16) u32 sm[REDUCE_BLOCK / 32][32];
+    const uint2 blk = r.blocks[blockIdx.x];
+    const WinDesc wd = r.wins[blk.x];
+    const u32 j = blk.y * REDUCE_BLOCK + threadIdx.x;
+    const u32 lo = j * wd.chunk;  // weights lo+1 .. lo+chunk
+    Xyzz sum = xyzz_identity(), sos = xyzz_identity();
+    if (lo < wd.nbuckets) {
+        const u32 hi = min(lo + wd.chunk, wd.nbuckets);
+        for (u32 k = hi; k > lo; k--) {
+            const u32 g = wd.bucket_base + k - 1;
+            if (r.offsets[g + 1] != r.offsets[g]) sum = xyzz_add(sum, xyzz_load(r.buckets + (size_t)g * 32));
+            sos = xyzz_add(sos, sum);
+        }
+        sos = xyzz_add(sos, xyzz_mul_u32(sum, lo));
+    }
+#pragma unroll 1
+    for (u32 o = 16; o; o >>= 1) sos = xyzz_add(sos, xyzz_shfl_down(sos, o));
+    const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    if (lane == 0) xyzz_store(&sm[wid][0], sos);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Xyzz acc = xyzz_load(&sm[0][0]);
+        for (u32 k = 1; k < REDUCE_BLOCK / 32; k++) acc = xyzz_add(acc, xyzz_load(&sm[k][0]));
+        xyzz_store(r.parts + (size_t)(wd.part_base + blk.y) * 32, acc);
+    }
+}
+
+struct FinalArgs {
+    const MsmDesc *descs;
+    const WinDesc *wins;
+    const u32 *parts;
+    u32 M;
+    u32 *carry;       // optional XYZZ per MSM: added in, or written when !emit_affine
+    int emit_affine;  // write canonical affine results
+    u32 *results;     // 16 u32 per MSM
+};
+
+__global__ void k_final(FinalArgs f) {
+    const u32 m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= f.M) return;
+    const MsmDesc d = f.descs[m];
+    Xyzz acc = xyzz_identity();
+    for (int pw = (int)d.n_windows - 1; pw >= 0; pw--) {
+        if (!xyzz_is_identity(acc))
+            for (u32 k = 0; k < d.c; k++) acc = xyzz_dbl(acc);
+        const WinDesc wd = f.wins[d.win_base + pw];
+        for (u32 p = 0; p < wd.nparts; p++) acc = xyzz_add(acc, xyzz_load(f.parts + (size_t)(wd.part_base + p) * 32));
+    }
+    if (f.carry) acc = xyzz_add(acc, xyzz_load(f.carry + (size_t)m * 32));
+    if (f.emit_affine) {
+        Affine r = xyzz_to_affine(acc);
+        affine_store(f.results + (size_t)m * 16, r);
+    } else {
+        xyzz_store(f.carry + (size_t)m * 32, acc);
+    }
+}
+
+// Sum of k XYZZ points (per-card partials) to canonical affine.
+__global__ void k_combine(const u32 *xyzz, u32 k, u32 *out) {
+    if (blockIdx.x || threadIdx.x) return;
+    Xyzz acc = xyzz_identity();
+    for (u32 i = 0; i < k; i++) acc = xyzz_add(acc, xyzz_load(xyzz + (size_t)i * 32));
+    affine_store(out, xyzz_to_affine(acc));
+}
+
+}  // namespace impeller

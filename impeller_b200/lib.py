@@ -1,0 +1,110 @@
+"""ctypes bindings of libimpeller_msm.so (the C ABI in include/impeller_msm.h).
+
+There is no fallback: if the CUDA library is missing or fails to load, every
+entry point raises.  The library is built in-tree by ``impeller_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libimpeller_msm.so")
+
+c_u32p = ctypes.POINTER(ctypes.c_uint32)
+c_u32pp = ctypes.POINTER(c_u32p)
+c_void_pp = ctypes.POINTER(ctypes.c_void_p)
+c_ulong_p = ctypes.POINTER(ctypes.c_ulong)
+
+# Every symbol include/impeller_msm.h declares, with (restype, argtypes).
+SIGNATURES: dict[str, tuple] = {
+    "msm": (ctypes.c_int, [c_void_pp, c_ulong_p, ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
+                           ctypes.c_uint, ctypes.c_uint, c_u32p, c_u32pp, ctypes.c_uint, c_u32pp, c_u32pp]),
+    "msm_precompute": (ctypes.c_int, [ctypes.c_ulonglong, c_u32pp, ctypes.c_uint]),
+    "impeller_msm_cfg": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, ctypes.c_int, c_void_pp, c_ulong_p,
+                                        ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
+                                        ctypes.c_uint, ctypes.c_uint, c_u32p, c_u32pp, ctypes.c_uint, c_u32pp,
+                                        c_u32pp]),
+    "impeller_msm_precompute_cfg": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, ctypes.c_ulonglong, c_u32pp,
+                                                   ctypes.c_uint]),
+    "impeller_msm_n_precompute": (ctypes.c_uint, [ctypes.c_uint, ctypes.c_uint]),
+    "impeller_ctx_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.c_uint64, ctypes.c_int]),
+    "impeller_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "impeller_ctx_points": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "impeller_ctx_len": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "impeller_default_window": (ctypes.c_uint, [ctypes.c_uint64]),
+    "impeller_set_window_table": (ctypes.c_int, [c_u32p, c_u32p, ctypes.c_uint32]),
+    "impeller_msm_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint,
+                                           ctypes.c_void_p, ctypes.c_void_p]),
+    "impeller_msm_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
+    "impeller_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p,
+                                             ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint),
+                                             ctypes.c_uint32, ctypes.c_uint32]),
+    "impeller_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "impeller_batch_run": (ctypes.c_int, [ctypes.c_void_p, c_void_pp, ctypes.c_void_p, ctypes.c_void_p]),
+    "impeller_batch_launches": (ctypes.c_uint32, [ctypes.c_void_p]),
+    "impeller_gen_scalars": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                            ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
+    "impeller_gen_points": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                           ctypes.c_void_p]),
+    "impeller_test_field_op": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
+    "impeller_test_point_op": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_uint64, ctypes.c_void_p]),
+    "impeller_ctx_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "impeller_ctx_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_uint32,
+                                                 ctypes.POINTER(ctypes.c_uint32)]),
+    "impeller_phase_name": (ctypes.c_char_p, [ctypes.c_uint32]),
+    "impeller_imad_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "impeller_last_error": (ctypes.c_char_p, []),
+    "impeller_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+class ImpellerError(RuntimeError):
+    pass
+
+
+def load(path: str | None = None):
+    """Load the CUDA library (once).  Raises if it is not built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImpellerError(f"{p} is missing: build it with `python -m impeller_b200.build` "
+                            "(there is no CPU fallback)")
+    L = ctypes.CDLL(p, mode=ctypes.RTLD_GLOBAL)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = L
+    return L
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != 0:
+        msg = load().impeller_last_error().decode(errors="replace")
+        raise ImpellerError(f"{what or 'impeller call'} failed with cudaError {rc}: {msg}")
+
+
+def declared_symbols(header: str | None = None) -> list[str]:
+    """Function names declared in include/impeller_msm.h."""
+    import re
+    header = header or os.path.join(os.path.dirname(HERE), "include", "impeller_msm.h")
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"\b([A-Za-z_]\w*)\s*\(", text)
+    keep = []
+    for n in names:
+        if n in ("if", "sizeof", "defined") or n.isupper():
+            continue
+        if n not in keep:
+            keep.append(n)
+    return [n for n in keep if n.startswith(("msm", "impeller_"))]

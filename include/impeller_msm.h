@@ -1,0 +1,160 @@
+/*
+ * impeller_msm.h -- C ABI of libimpeller_msm.so, the B200 (sm_100a) BN254 G1
+ * multi-scalar multiplication.
+ *
+ * Data layout everywhere (the reference's, core/src/msm/src/msm.h and
+ * core/src/msm.rs:319-341): a field element is 8 little-endian uint32 limbs in
+ * Montgomery form (R = 2^256); an affine point is 16 uint32 (x then y),
+ * byte-identical to halo2curves' G1Affine; the identity point is (0, 0).
+ * Scalars are Fr elements in Montgomery form.  Results are canonical affine
+ * points in the same form.
+ *
+ * Return values are cudaError_t codes; argument errors return
+ * cudaErrorInvalidValue and impeller_last_error() says why.
+ */
+#ifndef IMPELLER_MSM_H
+#define IMPELLER_MSM_H
+
+#include <cuda_runtime_api.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * Drop-in replacements of the reference's two symbols.
+ *
+ * Replaces core/src/msm/src/msm.h:4-9 (defined in core/src/msm/src/msm.cu:9-41),
+ * bound by core/src/msm.rs:116-133 and called at core/src/msm.rs:282-302
+ * (size query) and :349-365 (run).  Same two-phase protocol: with
+ * buffers == NULL the per-card scratch byte sizes are written to
+ * buffer_sizes[0..num_cards) and nothing runs; otherwise buffers[i] is a
+ * device allocation of at least that size on card cards[i].  h_points holds
+ * n_precompute host arrays of len points (table j = 2^(j*n_windows*c) * P),
+ * h_scaler_batch holds `batches` host arrays of len scalars, h_result
+ * `batches` host arrays of 16 uint32.  Blocking, like the reference.
+ *
+ * The window size c and target window count of this symbol are those of the
+ * library it is loaded from: 16 and 16 for libimpeller_msm.so (the
+ * reference's MsmConfig::default, common/src/msm_config.rs:52-55), or the
+ * values baked into a per-configuration shim named like the reference's
+ * libmsm_bn254_{c}_{alpha}_{debug}.so (core/src/msm.rs:101-112).
+ */
+cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, unsigned long long len,
+                unsigned int batch_per_run, unsigned int parts, unsigned int stage_scalers,
+                unsigned int stage_points, unsigned int num_cards, const unsigned int *cards,
+                unsigned int const *const *h_points, unsigned int batches,
+                unsigned int const *const *h_scaler_batch, unsigned int *const *h_result);
+
+/* Replaces core/src/msm/src/msm.h:11 (core/src/msm/src/msm.cu:43-49,
+ * MSMPrecompute::precompute at core/src/msm/src/msm_impl.cuh:803-829), bound
+ * by core/src/msm.rs:139-146.  Fills h_points[1..n_precompute) from
+ * h_points[0] on up to max_cards devices. */
+cudaError_t msm_precompute(unsigned long long len, unsigned int *const *h_points, unsigned int max_cards);
+
+/* The same two entry points with the configuration as arguments (the
+ * reference bakes window_size / target_window into the library name,
+ * core/src/msm.rs:101-112; per-configuration shims forward here). */
+cudaError_t impeller_msm_cfg(unsigned int window_size, unsigned int target_window, int debug,
+                             void *const *buffers, unsigned long *buffer_sizes, unsigned long long len,
+                             unsigned int batch_per_run, unsigned int parts, unsigned int stage_scalers,
+                             unsigned int stage_points, unsigned int num_cards, const unsigned int *cards,
+                             unsigned int const *const *h_points, unsigned int batches,
+                             unsigned int const *const *h_scaler_batch, unsigned int *const *h_result);
+cudaError_t impeller_msm_precompute_cfg(unsigned int window_size, unsigned int target_window,
+                                        unsigned long long len, unsigned int *const *h_points,
+                                        unsigned int max_cards);
+
+/* Number of window tables the reference derives from (window_size,
+ * target_window) for a 254-bit scalar (common/src/msm_config.rs:17-25). */
+unsigned int impeller_msm_n_precompute(unsigned int window_size, unsigned int target_window);
+
+/* ------------------------------------------------------------------------
+ * Resident-SRS context (additive; no reference counterpart -- the reference
+ * re-uploads its points on every call, core/src/msm/src/msm_impl.cuh:478-499).
+ */
+typedef struct impeller_ctx impeller_ctx;
+
+/* Upload (or adopt) `len` affine points to `device`.  points_on_device != 0
+ * means `points` is already a device pointer on that device; the context then
+ * borrows it and the caller keeps it alive. */
+cudaError_t impeller_ctx_create(impeller_ctx **out, int device, const uint32_t *points, uint64_t len,
+                                int points_on_device);
+cudaError_t impeller_ctx_destroy(impeller_ctx *ctx);
+/* Device pointer of the resident points (len x 16 uint32). */
+const uint32_t *impeller_ctx_points(const impeller_ctx *ctx);
+uint64_t impeller_ctx_len(const impeller_ctx *ctx);
+
+/* Window size the autotune table picks for an MSM of n points (0 -> none). */
+unsigned int impeller_default_window(uint64_t n);
+/* Load an autotune table: `count` pairs (log2 n, c); nearest log2 n wins. */
+cudaError_t impeller_set_window_table(const uint32_t *log2n, const uint32_t *c, uint32_t count);
+
+/* One MSM over the first n resident points.  d_scalars: device, n x 8
+ * uint32 (Montgomery Fr); d_result: device, 16 uint32.  c == 0 picks the
+ * window from the table.  Asynchronous on `stream`. */
+cudaError_t impeller_msm_device(impeller_ctx *ctx, const uint32_t *d_scalars, uint64_t n, unsigned int c,
+                                uint32_t *d_result, cudaStream_t stream);
+/* Same with host scalars and result: copies in, runs, copies out, waits. */
+cudaError_t impeller_msm_host(impeller_ctx *ctx, const uint32_t *h_scalars, uint64_t n, unsigned int c,
+                              uint32_t *h_result, cudaStream_t stream);
+
+/* Per-phase timing of a context's MSMs: when enabled, each run records CUDA
+ * events on its stream between phases (tables, histogram, scan, scatter,
+ * accumulate, fixup, reduce, final).  profile_read waits for the recorded
+ * runs, writes the summed milliseconds of each phase (nphase >= 8) and the
+ * number of runs, and clears the record. */
+cudaError_t impeller_ctx_profile(impeller_ctx *ctx, int enable);
+cudaError_t impeller_ctx_profile_read(impeller_ctx *ctx, double *ms_per_phase, uint32_t nphase, uint32_t *runs);
+const char *impeller_phase_name(uint32_t i);
+
+/* ------------------------------------------------------------------------
+ * Batched MSMs of uneven sizes over prefixes of the resident points: one
+ * plan, every phase one launch for the whole batch, optionally captured in a
+ * CUDA graph and replayed.  sizes[i] <= ctx len; windows[i] == 0 picks the
+ * table's window; windows may be NULL.
+ */
+typedef struct impeller_batch impeller_batch;
+#define IMPELLER_BATCH_GRAPH 1u
+cudaError_t impeller_batch_create(impeller_batch **out, impeller_ctx *ctx, const uint64_t *sizes,
+                                  const unsigned int *windows, uint32_t count, uint32_t flags);
+cudaError_t impeller_batch_destroy(impeller_batch *b);
+/* d_scalars[i]: device scalars of MSM i; d_results: device, count x 16. */
+cudaError_t impeller_batch_run(impeller_batch *b, const uint32_t *const *d_scalars, uint32_t *d_results,
+                               cudaStream_t stream);
+/* Kernel launches one run of the batch issues (for launch accounting). */
+uint32_t impeller_batch_launches(const impeller_batch *b);
+
+/* ------------------------------------------------------------------------
+ * Seeded synthetic inputs, computed on the device (definitions shared with
+ * the CPU oracle: splitmix64 counter streams, uniform Fr, the skewed
+ * witness-like mix, P_i = r_i * G). */
+cudaError_t impeller_gen_scalars(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t stream, int dist,
+                                 uint64_t start, int mont, cudaStream_t s);
+cudaError_t impeller_gen_points(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t start, cudaStream_t s);
+
+/* Element-wise field / point operations on the device, for parity tests.
+ * field: 0 = Fq, 1 = Fr.  op: 0 add, 1 sub, 2 mul, 3 sqr, 4 neg, 5 to_mont,
+ * 6 from_mont, 7 inv, 8 pow.  Point ops (affine in/out): 0 add (madd path),
+ * 1 dbl, 2 add via XYZZ+XYZZ, 3 k*P (k plain 256-bit). */
+cudaError_t impeller_test_field_op(int field, int op, const uint32_t *d_a, const uint32_t *d_b, uint32_t *d_out,
+                                   uint64_t count, cudaStream_t s);
+cudaError_t impeller_test_point_op(int op, const uint32_t *d_p, const uint32_t *d_q, uint32_t *d_out,
+                                   uint64_t count, cudaStream_t s);
+
+/* Integer multiply-add peak of `device`, measured: independent mad.lo /
+ * mad.hi chains (the instruction mix of the Montgomery product), in 10^9
+ * multiply-add instructions per second.  Blocks until done. */
+cudaError_t impeller_imad_peak(int device, double *gops);
+
+/* Last error message of the calling thread ("" if none). */
+const char *impeller_last_error(void);
+/* Library version string. */
+const char *impeller_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMPELLER_MSM_H */
