@@ -118,7 +118,7 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
 
     // reduce: chunk length per thread, partial-sum slots per window
     const u64 target = (u64)sms * 512;
-    u32 L = 8;
+    u32 L = 16;
     while (nb / L > target && L < (1u << 30)) L <<= 1;
     std::vector<uint2> rblocks;
     u32 nparts = 0;
@@ -174,6 +174,8 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     lo.o_recb = take((size_t)2 * T * 4);
     lo.o_recp = take((size_t)2 * T * 128);
     lo.o_parts = take((size_t)nparts * 128);
+    lo.o_parts_s = take((size_t)nparts * 128);
+    lo.o_wres = take((size_t)wins.size() * 128);
     lo.o_long = take((size_t)(1 + p.long_cap) * 4);
     lo.o_carry = take((size_t)p.M * 128);
     lo.o_results = take((size_t)p.M * 64);
@@ -188,7 +190,7 @@ Plan::~Plan() {
         for (auto e : set) cudaEventDestroy(e);
 }
 
-u32 Plan::launches() const { return 10; }
+u32 Plan::launches() const { return 11; }
 
 const char *Plan::phase_name(int i) {
     static const char *names[NPHASE] = {"tables", "histogram", "scan", "scatter",
@@ -260,6 +262,8 @@ cudaError_t Plan::launch(void *scratch, const u32 *points, u32 *results, int car
     u32 *recb = reinterpret_cast<u32 *>(s + layout.o_recb);
     u32 *recp = reinterpret_cast<u32 *>(s + layout.o_recp);
     u32 *parts = reinterpret_cast<u32 *>(s + layout.o_parts);
+    u32 *parts_s = reinterpret_cast<u32 *>(s + layout.o_parts_s);
+    u32 *wres = reinterpret_cast<u32 *>(s + layout.o_wres);
     u32 *longl = reinterpret_cast<u32 *>(s + layout.o_long);
     u32 *carry = carry_ext ? carry_ext : reinterpret_cast<u32 *>(s + layout.o_carry);
     u32 *res = results ? results : reinterpret_cast<u32 *>(s + layout.o_results);
@@ -303,18 +307,16 @@ cudaError_t Plan::launch(void *scratch, const u32 *points, u32 *results, int car
     CK_LAUNCH("k_fixup_long");
     MARK(6);
 
-    ReduceArgs ra{d_wins, d_blk, offsets, buckets, parts};
+    ReduceArgs ra{d_wins, d_blk, offsets, buckets, parts, parts_s};
     k_reduce<<<nrblocks, REDUCE_BLOCK, 0, st>>>(ra);
     CK_LAUNCH("k_reduce");
     MARK(7);
 
-    if (carry_mode == 0) {
-        FinalArgs fa2{d_desc, d_wins, parts, M, nullptr, 1, res};
-        k_final<<<(M + 31) / 32, 32, 0, st>>>(fa2);
-    } else {
-        FinalArgs fa2{d_desc, d_wins, parts, M, carry, carry_mode == 1 ? 1 : 0, res};
-        k_final<<<(M + 31) / 32, 32, 0, st>>>(fa2);
-    }
+    WindowSumArgs wa{d_desc, d_wins, parts, parts_s, nwins, wres};
+    k_window_sum<<<(nwins + 3) / 4, 128, 0, st>>>(wa);
+    CK_LAUNCH("k_window_sum");
+    FinalArgs fa2{d_desc, wres, M, carry_mode == 0 ? nullptr : carry, carry_mode == 2 ? 0 : 1, res};
+    k_final<<<(M + 3) / 4, 128, 0, st>>>(fa2);
     CK_LAUNCH("k_final");
     MARK(8);
 #undef MARK
@@ -382,6 +384,17 @@ static u32 model_window(u64 n) {
     return best;
 }
 
+// With resident window tables of window c_tab, an MSM of n points costs
+// W(c_tab) * n mixed additions plus one bucket set of 2^(c_tab-1); without,
+// the cost model's best plain window.  Pick the cheaper.
+u32 tables_worthwhile(u64 n, u32 c_tab) {
+    if (c_tab == 0) return 0;
+    const u32 c = default_window(n);
+    const double plain = (double)digit_windows(c) * ((double)n * 10.0 + std::ldexp(1.0, (int)c - 1) * 45.0);
+    const double tab = (double)digit_windows(c_tab) * (double)n * 10.0 + std::ldexp(1.0, (int)c_tab - 1) * 45.0;
+    return tab < plain ? c_tab : 0;
+}
+
 u32 default_window(u64 n) {
     if (n == 0) return 0;
     std::lock_guard<std::mutex> g(g_tab_mu);
@@ -418,8 +431,18 @@ struct impeller_ctx {
     u32 *d_result = nullptr;
     cudaEvent_t done = nullptr;  // last run that used the scratch
     bool profiling = false;
+    u32 *tables = nullptr;       // W(table_c) window tables, table j = 2^(j*c) * P
+    u32 table_c = 0;
     std::map<std::pair<u32, u32>, std::unique_ptr<Plan>> plans;
 };
+
+static u32 ctx_window(const impeller_ctx *ctx, u64 n) {
+    if (ctx->tables) {
+        u32 c = tables_worthwhile(n, ctx->table_c);
+        if (c) return c;
+    }
+    return default_window(n);
+}
 
 static cudaError_t ctx_reserve(impeller_ctx *ctx, size_t bytes, cudaStream_t st) {
     if (bytes <= ctx->scratch_bytes) return cudaSuccess;
@@ -433,12 +456,21 @@ static cudaError_t ctx_reserve(impeller_ctx *ctx, size_t bytes, cudaStream_t st)
     return cudaSuccess;
 }
 
+// Shape of an MSM of n points with window c on this context: with resident
+// window tables for c every digit window shares one bucket set.
+static MsmShape ctx_shape(const impeller_ctx *ctx, u32 n, u32 c) {
+    if (ctx->tables && c == ctx->table_c) return MsmShape{n, c, 1, (u32)ctx->len};
+    return MsmShape{n, c, 0, 0};
+}
+
+static const u32 *ctx_point_base(const impeller_ctx *ctx) { return ctx->tables ? ctx->tables : ctx->points; }
+
 static Plan *ctx_plan(impeller_ctx *ctx, u32 n, u32 c) {
     auto key = std::make_pair(n, c);
     auto it = ctx->plans.find(key);
     if (it != ctx->plans.end()) return it->second.get();
     std::unique_ptr<Plan> p(new Plan());
-    if (!Plan::build(*p, ctx->device, {MsmShape{n, c, 0, 0}})) return nullptr;
+    if (!Plan::build(*p, ctx->device, {ctx_shape(ctx, n, c)})) return nullptr;
     Plan *raw = p.get();
     raw->set_profiling(ctx->profiling);
     ctx->plans[key] = std::move(p);
@@ -506,6 +538,7 @@ cudaError_t impeller_ctx_destroy(impeller_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
     if (ctx->owns) cudaFree(const_cast<u32 *>(ctx->points));
+    if (ctx->tables) cudaFree(ctx->tables);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_scalars) cudaFree(ctx->d_scalars);
     if (ctx->d_result) cudaFree(ctx->d_result);
@@ -516,6 +549,40 @@ cudaError_t impeller_ctx_destroy(impeller_ctx *ctx) {
 }
 
 const uint32_t *impeller_ctx_points(const impeller_ctx *ctx) { return ctx ? ctx->points : nullptr; }
+
+cudaError_t impeller_ctx_precompute(impeller_ctx *ctx, unsigned int c) {
+    if (!ctx || c < 3 || c > 31) {
+        set_error("impeller_ctx_precompute: window size must be in [3, 31]");
+        return cudaErrorInvalidValue;
+    }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaDeviceSynchronize());
+    const u32 W = digit_windows(c);
+    if ((u64)W * ctx->len >= (1ull << 31)) {
+        set_error("impeller_ctx_precompute: window tables exceed 2^31 points");
+        return cudaErrorInvalidValue;
+    }
+    if (ctx->tables) CK(cudaFree(ctx->tables));
+    ctx->tables = nullptr;
+    ctx->table_c = 0;
+    ctx->plans.clear();
+    u32 *t = nullptr;
+    CK(cudaMalloc(&t, (size_t)W * std::max<u64>(ctx->len, 1) * 64));
+    cudaError_t e = cudaMemcpy(t, ctx->points, ctx->len * 64, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = precompute_tables(t, ctx->len, c, W, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        cudaFree(t);
+        set_error(std::string("impeller_ctx_precompute: ") + cudaGetErrorString(e));
+        return e;
+    }
+    ctx->tables = t;
+    ctx->table_c = c;
+    return cudaSuccess;
+}
+
+unsigned int impeller_ctx_window(const impeller_ctx *ctx, uint64_t n) { return ctx ? ctx_window(ctx, n) : 0; }
 uint64_t impeller_ctx_len(const impeller_ctx *ctx) { return ctx ? ctx->len : 0; }
 
 static cudaError_t ctx_run_locked(impeller_ctx *ctx, const uint32_t *d_scalars, uint64_t n, unsigned int c,
@@ -525,7 +592,7 @@ static cudaError_t ctx_run_locked(impeller_ctx *ctx, const uint32_t *d_scalars, 
         return cudaErrorInvalidValue;
     }
     if (n == 0) return cudaMemsetAsync(d_result, 0, 64, stream);
-    if (c == 0) c = default_window(n);
+    if (c == 0) c = ctx_window(ctx, n);
     CK(cudaSetDevice(ctx->device));
     Plan *p = ctx_plan(ctx, (u32)n, c);
     if (!p) return cudaErrorInvalidValue;
@@ -533,7 +600,7 @@ static cudaError_t ctx_run_locked(impeller_ctx *ctx, const uint32_t *d_scalars, 
     if (e != cudaSuccess) return e;
     CK(cudaStreamWaitEvent(stream, ctx->done, 0));
     const u32 *sc[1] = {d_scalars};
-    e = p->enqueue(ctx->scratch, ctx->points, sc, d_result, 0, stream);
+    e = p->enqueue(ctx->scratch, ctx_point_base(ctx), sc, d_result, 0, stream);
     if (e != cudaSuccess) return e;
     CK(cudaEventRecord(ctx->done, stream));
     return cudaSuccess;
@@ -634,8 +701,8 @@ cudaError_t impeller_batch_create(impeller_batch **out, impeller_ctx *ctx, const
             set_error("impeller_batch_create: size 0 or larger than the resident point array");
             return cudaErrorInvalidValue;
         }
-        u32 c = windows && windows[i] ? windows[i] : default_window(sizes[i]);
-        shapes.push_back(MsmShape{(u32)sizes[i], c, 0, 0});
+        u32 c = windows && windows[i] ? windows[i] : ctx_window(ctx, sizes[i]);
+        shapes.push_back(ctx_shape(ctx, (u32)sizes[i], c));
     }
     std::unique_ptr<impeller_batch> b(new impeller_batch());
     b->ctx = ctx;
@@ -671,13 +738,13 @@ cudaError_t impeller_batch_run(impeller_batch *b, const uint32_t *const *d_scala
     cudaError_t e = b->plan.stage(d_scalars);
     if (e != cudaSuccess) return e;
     if (!b->graph) {
-        e = b->plan.launch(b->scratch, b->ctx->points, nullptr, 0, stream);
+        e = b->plan.launch(b->scratch, ctx_point_base(b->ctx), nullptr, 0, stream);
         if (e != cudaSuccess) return e;
     } else {
         if (!b->exec) {
             CK(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
             CK(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
-            e = b->plan.launch(b->scratch, b->ctx->points, nullptr, 0, b->cap_stream, nullptr, false);
+            e = b->plan.launch(b->scratch, ctx_point_base(b->ctx), nullptr, 0, b->cap_stream, nullptr, false);
             cudaGraph_t g = nullptr;
             cudaError_t e2 = cudaStreamEndCapture(b->cap_stream, &g);
             if (e != cudaSuccess) return e;

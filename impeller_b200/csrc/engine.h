@@ -33,7 +33,7 @@ int sm_count(int device);
 struct PlanLayout {
     size_t o_tables, tables_bytes;  // descs | wins | reduce blocks (uploaded each run)
     size_t o_counts, o_cursor, o_offsets, o_tiles, o_entries, o_buckets;
-    size_t o_recb, o_recp, o_parts, o_long, o_carry, o_results;
+    size_t o_recb, o_recp, o_parts, o_parts_s, o_wres, o_long, o_carry, o_results;
     size_t bytes;
 };
 

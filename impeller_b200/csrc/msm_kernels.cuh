@@ -13,8 +13,11 @@
 //                 boundary leave partial sums                  [IMAD-bound]
 //   k_fixup_*     merge the partial sums of cut buckets (short runs per
 //                 thread, long runs -- heavy buckets -- per warp)
-//   k_reduce      per window sum_k k * S_k by chunked running sums
-//   k_final       per MSM Horner combine of the windows, affine conversion
+//   k_reduce      per window sum_k k * S_k by chunked running sums whose
+//                 cross-chunk weights come from a suffix scan
+//   k_window_sum  per window (one warp): finish the window total, weight it
+//                 by 2^(c * window)
+//   k_final       per MSM (one warp): sum the windows, affine conversion
 //
 // Differences from the reference (core/src/msm/src/msm_impl.cuh): the
 // reference sorts 64-bit keys with CUB radix sort (:459-463), protects the
@@ -353,24 +356,38 @@ __global__ void k_fixup_long(FixupArgs f) {
 }
 
 // ----------------------------------------------------------------- reduce
+//
+// Window total T = sum_{k=1..B} k * S_k.  Thread j of a window owns the
+// weights (jL, (j+1)L] and forms by a running sum from the top
+//   sum_j = sum_k S_k   and   sos_j = sum_k (k - jL) * S_k.
+// Since sum_j j * sum_j = sum_{i>=1} suffix_i with suffix_i = sum_{j>=i} sum_j,
+//   T = sum_j (sos_j + L * suffix_{j+1}),
+// so each thread needs only the exclusive suffix of the chunk sums (a scan)
+// and log2(L) doublings -- no per-thread scalar multiplication.  Inside a
+// block of 128 threads the suffix is a warp shuffle scan; the part owed to
+// later blocks of the window is sum_b b * S_b over the block totals S_b,
+// scaled by 128 L, and is added by k_window_sum.
 
 struct ReduceArgs {
     const WinDesc *wins;
     const uint2 *blocks;  // (window, block-in-window) per reduce block
     const u32 *offsets;
     const u32 *buckets;
-    u32 *parts;           // XYZZ partial per reduce block
+    u32 *parts_v;         // XYZZ per reduce block: sum_j (sos_j + L * local suffix_{j+1})
+    u32 *parts_s;         // XYZZ per reduce block: block total of sum_j
 };
 
 static constexpr u32 REDUCE_BLOCK = 128;
+static constexpr u32 REDUCE_WARPS = REDUCE_BLOCK / 32;
 
-// Thread j of window w sums the chunk of weights (j*L, (j+1)*L]:
-// running sums from the top give sum_k (k - j*L) * S_k and sum_k S_k;
-// adding (j*L) * sum_k S_k gives the chunk's share of sum_k k * S_k.
+__device__ __forceinline__ u32 ilog2(u32 x) { return 31 - __clz(x); }
+
 __global__ void __launch_bounds__(REDUCE_BLOCK) k_reduce(ReduceArgs r) {
-    __shared__ __align__(16) u32 sm[REDUCE_BLOCK / 32][32];
+    __shared__ __align__(16) u32 sm_tot[REDUCE_WARPS][32];
+    __shared__ __align__(16) u32 sm_v[REDUCE_WARPS][32];
     const uint2 blk = r.blocks[blockIdx.x];
     const WinDesc wd = r.wins[blk.x];
+    const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     const u32 j = blk.y * REDUCE_BLOCK + threadIdx.x;
     const u32 lo = j * wd.chunk;  // weights lo+1 .. lo+chunk
     Xyzz sum = xyzz_identity(), sos = xyzz_identity();
@@ -381,41 +398,116 @@ __global__ void __launch_bounds__(REDUCE_BLOCK) k_reduce(ReduceArgs r) {
             if (r.offsets[g + 1] != r.offsets[g]) sum = xyzz_add(sum, xyzz_load(r.buckets + (size_t)g * 32));
             sos = xyzz_add(sos, sum);
         }
-        sos = xyzz_add(sos, xyzz_mul_u32(sum, lo));
     }
+    // inclusive suffix of `sum` inside the warp
+    Xyzz x = sum;
 #pragma unroll 1
-    for (u32 o = 16; o; o >>= 1) sos = xyzz_add(sos, xyzz_shfl_down(sos, o));
-    const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-    if (lane == 0) xyzz_store(&sm[wid][0], sos);
+    for (u32 o = 1; o < 32; o <<= 1) {
+        Xyzz y = xyzz_shfl_down(x, o);
+        if (lane + o < 32) x = xyzz_add(x, y);
+    }
+    if (lane == 0) xyzz_store(&sm_tot[wid][0], x);
+    __syncthreads();
+    Xyzz later = xyzz_identity();  // totals of the later warps of this block
+    for (u32 w2 = wid + 1; w2 < REDUCE_WARPS; w2++) later = xyzz_add(later, xyzz_load(&sm_tot[w2][0]));
+    Xyzz ex = xyzz_shfl_down(x, 1);
+    if (lane == 31) ex = xyzz_identity();
+    ex = xyzz_add(ex, later);
+    const u32 lg = ilog2(wd.chunk);
+    for (u32 k = 0; k < lg; k++) ex = xyzz_dbl(ex);
+    Xyzz v = xyzz_add(sos, ex);
+#pragma unroll 1
+    for (u32 o = 16; o; o >>= 1) v = xyzz_add(v, xyzz_shfl_down(v, o));
+    if (lane == 0) xyzz_store(&sm_v[wid][0], v);
     __syncthreads();
     if (threadIdx.x == 0) {
-        Xyzz acc = xyzz_load(&sm[0][0]);
-        for (u32 k = 1; k < REDUCE_BLOCK / 32; k++) acc = xyzz_add(acc, xyzz_load(&sm[k][0]));
-        xyzz_store(r.parts + (size_t)(wd.part_base + blk.y) * 32, acc);
+        Xyzz acc = xyzz_load(&sm_v[0][0]);
+        Xyzz tot = xyzz_load(&sm_tot[0][0]);
+        for (u32 k = 1; k < REDUCE_WARPS; k++) {
+            acc = xyzz_add(acc, xyzz_load(&sm_v[k][0]));
+            tot = xyzz_add(tot, xyzz_load(&sm_tot[k][0]));
+        }
+        xyzz_store(r.parts_v + (size_t)(wd.part_base + blk.y) * 32, acc);
+        xyzz_store(r.parts_s + (size_t)(wd.part_base + blk.y) * 32, tot);
+    }
+}
+
+struct WindowSumArgs {
+    const MsmDesc *descs;
+    const WinDesc *wins;
+    const u32 *parts_v;
+    const u32 *parts_s;
+    u32 nwins;
+    u32 *wres;  // XYZZ per window: 2^(c * pw) * T
+};
+
+// One warp per window: T = sum_b V_b + 128 L * sum_b b * S_b, then weighted by
+// 2^(c * physical window) so the MSM result is the plain sum of its windows.
+__global__ void k_window_sum(WindowSumArgs a) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 win = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (win >= a.nwins) return;
+    const WinDesc wd = a.wins[win];
+    const MsmDesc d = a.descs[wd.msm];
+    const u32 pw = win - d.win_base;
+    // lane l owns a group of g block partials (g a power of two)
+    u32 g = 1;
+    while (g * 32 < wd.nparts) g <<= 1;
+    const u32 b0 = lane * g;
+    Xyzz vsum = xyzz_identity(), ssum = xyzz_identity(), sos = xyzz_identity();
+    for (u32 b = min(b0 + g, wd.nparts); b > b0; b--) {
+        const size_t slot = (size_t)(wd.part_base + b - 1) * 32;
+        vsum = xyzz_add(vsum, xyzz_load(a.parts_v + slot));
+        ssum = xyzz_add(ssum, xyzz_load(a.parts_s + slot));
+        sos = xyzz_add(sos, ssum);  // sum (b - b0) * S_b over the group
+    }
+    // sum_b b * S_b = sum_l (sos_l + g * suffix_{l+1}) over lanes
+    Xyzz x = ssum;
+#pragma unroll 1
+    for (u32 o = 1; o < 32; o <<= 1) {
+        Xyzz y = xyzz_shfl_down(x, o);
+        if (lane + o < 32) x = xyzz_add(x, y);
+    }
+    Xyzz ex = xyzz_shfl_down(x, 1);
+    if (lane == 31) ex = xyzz_identity();
+    for (u32 k = 0, lg = ilog2(g); k < lg; k++) ex = xyzz_dbl(ex);
+    Xyzz rs = xyzz_add(sos, ex);
+#pragma unroll 1
+    for (u32 o = 16; o; o >>= 1) {
+        rs = xyzz_add(rs, xyzz_shfl_down(rs, o));
+        vsum = xyzz_add(vsum, xyzz_shfl_down(vsum, o));
+    }
+    if (lane == 0) {
+        const u32 shift = ilog2(wd.chunk) + ilog2(REDUCE_BLOCK);
+        for (u32 k = 0; k < shift; k++) rs = xyzz_dbl(rs);
+        Xyzz t = xyzz_add(vsum, rs);
+        const u32 dbls = d.c * pw;
+        if (!xyzz_is_identity(t))
+            for (u32 k = 0; k < dbls; k++) t = xyzz_dbl(t);
+        xyzz_store(a.wres + (size_t)win * 32, t);
     }
 }
 
 struct FinalArgs {
     const MsmDesc *descs;
-    const WinDesc *wins;
-    const u32 *parts;
+    const u32 *wres;
     u32 M;
     u32 *carry;       // optional XYZZ per MSM: added in, or written when !emit_affine
     int emit_affine;  // write canonical affine results
     u32 *results;     // 16 u32 per MSM
 };
 
+// One warp per MSM: sum of its weighted windows, the carry, affine form.
 __global__ void k_final(FinalArgs f) {
-    const u32 m = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 lane = threadIdx.x & 31u;
+    const u32 m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (m >= f.M) return;
     const MsmDesc d = f.descs[m];
     Xyzz acc = xyzz_identity();
-    for (int pw = (int)d.n_windows - 1; pw >= 0; pw--) {
-        if (!xyzz_is_identity(acc))
-            for (u32 k = 0; k < d.c; k++) acc = xyzz_dbl(acc);
-        const WinDesc wd = f.wins[d.win_base + pw];
-        for (u32 p = 0; p < wd.nparts; p++) acc = xyzz_add(acc, xyzz_load(f.parts + (size_t)(wd.part_base + p) * 32));
-    }
+    for (u32 w = lane; w < d.n_windows; w += 32) acc = xyzz_add(acc, xyzz_load(f.wres + (size_t)(d.win_base + w) * 32));
+#pragma unroll 1
+    for (u32 o = 16; o; o >>= 1) acc = xyzz_add(acc, xyzz_shfl_down(acc, o));
+    if (lane != 0) return;
     if (f.carry) acc = xyzz_add(acc, xyzz_load(f.carry + (size_t)m * 32));
     if (f.emit_affine) {
         Affine r = xyzz_to_affine(acc);

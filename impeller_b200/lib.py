@@ -33,6 +33,8 @@ SIGNATURES: dict[str, tuple] = {
     "impeller_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "impeller_ctx_points": (ctypes.c_void_p, [ctypes.c_void_p]),
     "impeller_ctx_len": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "impeller_ctx_precompute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint]),
+    "impeller_ctx_window": (ctypes.c_uint, [ctypes.c_void_p, ctypes.c_uint64]),
     "impeller_default_window": (ctypes.c_uint, [ctypes.c_uint64]),
     "impeller_set_window_table": (ctypes.c_int, [c_u32p, c_u32p, ctypes.c_uint32]),
     "impeller_msm_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint,

@@ -310,6 +310,13 @@ class MsmContext:
         self.handle = h
         self.len = n
 
+    def precompute(self, c: int) -> None:
+        """Keep W(c) window tables (2^(j*c) * P) resident for window c."""
+        _lib.check(_lib.load().impeller_ctx_precompute(self.handle, c), "impeller_ctx_precompute")
+
+    def window(self, n: int) -> int:
+        return int(_lib.load().impeller_ctx_window(self.handle, n))
+
     def close(self) -> None:
         if self.handle:
             _lib.load().impeller_ctx_destroy(self.handle)

@@ -86,6 +86,16 @@ cudaError_t impeller_ctx_destroy(impeller_ctx *ctx);
 const uint32_t *impeller_ctx_points(const impeller_ctx *ctx);
 uint64_t impeller_ctx_len(const impeller_ctx *ctx);
 
+/* Resident window tables for window size c (additive; the device-resident
+ * counterpart of msm_precompute with one bucket set): W(c) = ceil(254/c)
+ * tables of len points, table j = 2^(j*c) * P, kept in HBM next to the points.
+ * MSMs on this context that use window c then accumulate every digit window
+ * into one bucket set: no per-window reduction and no window doublings.
+ * Replaces any previous tables.  Blocks until the tables are built. */
+cudaError_t impeller_ctx_precompute(impeller_ctx *ctx, unsigned int c);
+/* Window an MSM of n points uses on this context when c == 0 is passed. */
+unsigned int impeller_ctx_window(const impeller_ctx *ctx, uint64_t n);
+
 /* Window size the autotune table picks for an MSM of n points (0 -> none). */
 unsigned int impeller_default_window(uint64_t n);
 /* Load an autotune table: `count` pairs (log2 n, c); nearest log2 n wins. */

@@ -296,3 +296,21 @@ def test_reference_abi_rejects_bad_arguments(M):
     op = M.MSM(M.MsmConfig(parts=0))
     with pytest.raises(M._lib.ImpellerError):
         op.get_buffer_size(100)
+
+
+def test_resident_window_tables(M):
+    n = 20000
+    pts = O.gen_points(n, seed=21)
+    ctx = _ctx(M, pts)
+    ctx.precompute(10)
+    for m, c in ((n, 10), (n, 0), (777, 10), (n, 7), (1, 10)):
+        sc = O.gen_scalars(m, seed=21, stream=m + c)
+        assert (host(ctx.msm_device(dev(sc), n=m, c=c)) == O.msm(pts[:m], sc)).all(), (m, c)
+    sizes = [5, 300, 9000, n]
+    b = ctx.batch(sizes, windows=[10, 0, 10, 0], graph=True)
+    scal = [O.gen_scalars(s, seed=21, stream=500 + i) for i, s in enumerate(sizes)]
+    out = host(b.run([dev(s) for s in scal])).reshape(-1, 16)
+    for i, s in enumerate(sizes):
+        assert (out[i] == O.msm(pts[:s], scal[i])).all(), s
+    b.close()
+    ctx.close()
