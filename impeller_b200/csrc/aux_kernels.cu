@@ -192,6 +192,30 @@ __global__ void k_imad_peak(u32 *out, u32 iters, u32 seed) {
     if (x == 0x12345678u) out[blockIdx.x * blockDim.x + threadIdx.x] = x;
 }
 
+// Dependent chains of one operation on one thread (op 0 Fq product,
+// 1 XYZZ addition, 2 XYZZ doubling, 3 mixed addition), for latency numbers.
+__global__ void k_op_latency(int op, u32 iters, u32 *out, long long *cycles) {
+    Fq a = fe_one<FqP>();
+    a.l[0] ^= 0x1234567u;
+    Affine q;
+    q.x = fe_one<FqP>();
+    q.y = fe_add<FqP>(q.x, q.x);
+    Xyzz p = xyzz_from_affine(q);
+    p = xyzz_dbl(p);
+    long long t0 = clock64();
+    for (u32 i = 0; i < iters; i++) {
+        switch (op) {
+        case 0: a = fe_mul<FqP>(a, a); break;
+        case 1: p = xyzz_add(p, xyzz_dbl(p)); break;
+        case 2: p = xyzz_dbl(p); break;
+        default: p = xyzz_add_affine(p, q); break;
+        }
+    }
+    long long t1 = clock64();
+    out[0] = a.l[0] ^ p.x.l[0];
+    *cycles = t1 - t0;
+}
+
 cudaError_t launched(const char *what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) impeller::set_error(std::string("launch of ") + what + " failed: " + cudaGetErrorString(e));
@@ -255,6 +279,26 @@ cudaError_t impeller_imad_peak(int device, double *gops) {
     cudaFree(out);
     if (e != cudaSuccess) return e;
     *gops = (double)blocks * threads * iters * 16.0 / (best * 1e-3) / 1e9;
+    return cudaSuccess;
+}
+
+cudaError_t impeller_op_latency(int op, uint32_t iters, double *cycles_per_op) {
+    if (!cycles_per_op || iters == 0) return cudaErrorInvalidValue;
+    u32 *out = nullptr;
+    long long *cyc = nullptr;
+    cudaError_t e = cudaMalloc(&out, 64);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMalloc(&cyc, 8)) != cudaSuccess) {
+        cudaFree(out);
+        return e;
+    }
+    k_op_latency<<<1, 1>>>(op, iters, out, cyc);
+    long long h = 0;
+    e = cudaMemcpy(&h, cyc, 8, cudaMemcpyDeviceToHost);
+    cudaFree(out);
+    cudaFree(cyc);
+    if (e != cudaSuccess) return e;
+    *cycles_per_op = (double)h / iters;
     return cudaSuccess;
 }
 

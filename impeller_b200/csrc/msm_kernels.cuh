@@ -454,12 +454,15 @@ __global__ void k_window_sum(WindowSumArgs a) {
     u32 g = 1;
     while (g * 32 < wd.nparts) g <<= 1;
     const u32 b0 = lane * g;
+    // group-local weights: partial b carries weight b - b0, so the running
+    // sum adds into `sos` before each step down and not after the last one
     Xyzz vsum = xyzz_identity(), ssum = xyzz_identity(), sos = xyzz_identity();
-    for (u32 b = min(b0 + g, wd.nparts); b > b0; b--) {
+    const u32 top = min(b0 + g, wd.nparts);
+    for (u32 b = top; b > b0; b--) {
         const size_t slot = (size_t)(wd.part_base + b - 1) * 32;
+        if (b < top) sos = xyzz_add(sos, ssum);  // sum (b' - b0) * S_b' over the group
         vsum = xyzz_add(vsum, xyzz_load(a.parts_v + slot));
         ssum = xyzz_add(ssum, xyzz_load(a.parts_s + slot));
-        sos = xyzz_add(sos, ssum);  // sum (b - b0) * S_b over the group
     }
     // sum_b b * S_b = sum_l (sos_l + g * suffix_{l+1}) over lanes
     Xyzz x = ssum;

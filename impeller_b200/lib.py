@@ -60,6 +60,7 @@ SIGNATURES: dict[str, tuple] = {
                                                  ctypes.POINTER(ctypes.c_uint32)]),
     "impeller_phase_name": (ctypes.c_char_p, [ctypes.c_uint32]),
     "impeller_imad_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "impeller_op_latency": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
     "impeller_last_error": (ctypes.c_char_p, []),
     "impeller_version": (ctypes.c_char_p, []),
 }

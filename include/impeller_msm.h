@@ -158,6 +158,11 @@ cudaError_t impeller_test_point_op(int op, const uint32_t *d_p, const uint32_t *
  * multiply-add instructions per second.  Blocks until done. */
 cudaError_t impeller_imad_peak(int device, double *gops);
 
+/* Single-thread latency, in SM clock cycles, of a dependent chain of one
+ * operation: 0 Fq Montgomery product, 1 XYZZ addition (plus the doubling
+ * that feeds it), 2 XYZZ doubling, 3 mixed XYZZ + affine addition. */
+cudaError_t impeller_op_latency(int op, uint32_t iters, double *cycles_per_op);
+
 /* Last error message of the calling thread ("" if none). */
 const char *impeller_last_error(void);
 /* Library version string. */
