@@ -163,6 +163,28 @@ cudaError_t impeller_imad_peak(int device, double *gops);
  * that feeds it), 2 XYZZ doubling, 3 mixed XYZZ + affine addition. */
 cudaError_t impeller_op_latency(int op, uint32_t iters, double *cycles_per_op);
 
+/* ------------------------------------------------------------------------
+ * MSM that allocates nothing (no counterpart in the reference).
+ *
+ * For callers that cannot call cudaMalloc when they need an MSM: runtimes
+ * whose device memory is planned ahead of time into a fixed arena, paths
+ * where cudaMalloc / cudaFree would synchronize the device, processes that
+ * must not grow their device footprint after start-up.  All scratch comes
+ * from a file-scope __device__ array of IMPELLER_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading this library holds until exit; no device or pinned
+ * memory is allocated per call.  The caller passes the inputs (d_points:
+ * n affine points, d_scalars: n Montgomery Fr scalars, both device memory on
+ * the current device) and the output (d_result: 16 uint32, canonical affine).
+ * n > IMPELLER_NOALLOC_MAX_N returns cudaErrorInvalidValue.  Every call shares
+ * the one array, so calls that overlap on the GPU race: serialize them.  The
+ * first call on a device looks up the array's address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Asynchronous on `stream`.
+ */
+#define IMPELLER_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define IMPELLER_NOALLOC_MAX_N (1u << 14)
+cudaError_t impeller_msm_device_noalloc(const uint32_t *d_points, const uint32_t *d_scalars, uint64_t n,
+                                        uint32_t *d_result, cudaStream_t stream);
+
 /* Last error message of the calling thread ("" if none). */
 const char *impeller_last_error(void);
 /* Library version string. */
