@@ -97,15 +97,17 @@ class ClockSampler:
 
 # ----------------------------------------------------------- algorithmics
 
-def signed_digit_stats(scalars_canonical: np.ndarray, c: int) -> tuple[int, int]:
+def signed_digit_stats(scalars_canonical: np.ndarray, c: int, shared: bool = False) -> tuple[int, int]:
     """(nonzero signed digits, nonempty buckets) of the engine's recoding for
-    canonical scalars (n x 8 u32): the entry count of the accumulate phase."""
+    canonical scalars (n x 8 u32): the entry count of the accumulate phase.
+    shared: every digit window uses one bucket set (resident window tables)."""
     s = scalars_canonical.astype(np.uint64)
     words = [s[:, 2 * k] | (s[:, 2 * k + 1] << np.uint64(32)) for k in range(4)]
     W = math.ceil(254 / c)
     half = 1 << (c - 1)
     carry = np.zeros(s.shape[0], dtype=np.int64)
     nonzero, buckets = 0, 0
+    used = set()
     for w in range(W):
         o = w * c
         k, sh = divmod(o, 64)
@@ -121,8 +123,11 @@ def signed_digit_stats(scalars_canonical: np.ndarray, c: int) -> tuple[int, int]
             mag = d
         nz = mag != 0
         nonzero += int(nz.sum())
-        buckets += int(np.unique(mag[nz]).size)
-    return nonzero, buckets
+        if shared:
+            used.update(np.unique(mag[nz]).tolist())
+        else:
+            buckets += int(np.unique(mag[nz]).size)
+    return nonzero, (len(used) if shared else buckets)
 
 
 # One Fq Montgomery product issues 8 rows x (8 lo + 8 hi for a*b[i], 1 for
@@ -222,7 +227,12 @@ def main():
     V = 4  # rotating scalar vectors: 4 x 128 MiB + 256 MiB of points, inputs > L2
     scal = [M.gen_scalars_device(n, seed=0, stream_id=1 + v, device=dev) for v in range(V)]
     ctx = M.MsmContext(pts, device=dev)
-    c = M.default_window(n)
+    c_tab = M.table_window(n)  # resident window tables where the autotune table says they win
+    t0 = time.perf_counter()
+    if c_tab:
+        ctx.precompute(c_tab)
+    precompute_s = time.perf_counter() - t0
+    c = ctx.window(n)
     outs = [torch.empty(16, dtype=torch.int32, device=f"cuda:{dev}") for _ in range(V)]
 
     def barrier():
@@ -267,7 +277,7 @@ def main():
         # algorithmic work of the dominant kernel (accumulate) on the timed inputs
         canon = [M.to_host(M.gen_scalars_device(n, seed=0, stream_id=1 + v, mont=False, device=dev)).reshape(n, 8)
                  for v in range(V)]
-        stats = [signed_digit_stats(cv, c) for cv in canon]
+        stats = [signed_digit_stats(cv, c, shared=bool(c_tab)) for cv in canon]
         madds = statistics.mean(nz - nb for nz, nb in stats)
         entries = statistics.mean(nz for nz, _ in stats)
         peak = ctypes.c_double()
@@ -280,14 +290,17 @@ def main():
         except Exception:
             hbm_peak = 6650.0
         sort_ms = phase_ms["histogram"] + phase_ms["scan"] + phase_ms["scatter"]
-        sort_bytes = 2 * 32 * n + 4 * entries + 3 * 4 * (1 << (c - 1)) * math.ceil(254 / c)
+        nbk = (1 << (c - 1)) * (1 if c_tab else math.ceil(254 / c))
+        sort_bytes = 2 * 32 * n + 4 * entries + 3 * 4 * nbk
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32 (254-bit Montgomery, 8x32-bit limbs)",
             "data": "synthetic: P_i = r_i*G (r_i uniform Fr, seed 0), uniform Fr scalars (seeded streams)",
             "config": {"workload": f"plain single BN254 G1 MSM, n=2^{args.log2n}, window c={c} (autotune table)",
-                       "n": n, "window": c, "parallelism": f"replicas x{world}",
+                       "n": n, "window": c, "window_tables": bool(c_tab),
+                       "window_tables_setup_s": round(precompute_s, 3) if c_tab else None,
+                       "parallelism": f"replicas x{world}",
                        "l2": "inputs > L2: 256 MiB points + 4 rotating 128 MiB scalar vectors"},
             "gpu_launches": args.steps * 10,
             "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
@@ -322,7 +335,7 @@ def e2e_reference_abi(M, d_pts, d_scal, n, c, args) -> dict:
     """The reference's calling convention: host points and scalars (pinned),
     blocking msm() that uploads both, computes and returns the affine point."""
     import torch
-    cfg = M.MsmConfig(window_size=c, target_window=math.ceil(254 / c))
+    cfg = M.MsmConfig(window_size=c, target_window=math.ceil(254 / c))  # the drop-in path has no resident tables
     op = M.MSM(cfg)
     buf, keep = M.alloc_gpu_buffer(op.get_buffer_size(n)[0])
     hp = torch.empty((n, 16), dtype=torch.int32, pin_memory=True)

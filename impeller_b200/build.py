@@ -46,13 +46,25 @@ def _deps() -> list[str]:
     files = []
     for d in (CSRC, os.path.join(ROOT, "include")):
         for f in os.listdir(d):
-            if f.endswith((".cu", ".cuh", ".h", ".cpp")):
+            if f.endswith((".cu", ".cuh", ".h", ".cpp", ".inc")):
                 files.append(os.path.join(d, f))
     return files
 
 
+def write_default_table() -> None:
+    """csrc/autotune_default.inc from autotune_table.json (rewritten only when it changes)."""
+    sys.path.insert(0, ROOT)
+    from impeller_b200 import autotune
+    text = autotune.c_include()
+    path = os.path.join(CSRC, "autotune_default.inc")
+    if not os.path.exists(path) or open(path).read() != text:
+        with open(path, "w") as f:
+            f.write(text)
+
+
 def build(verbose: bool = False, ptxas_v: bool = False, force: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
+    write_default_table()
     deps = _deps()
     if not force and not _stale(LIB, deps + [os.path.abspath(__file__)]):
         return LIB

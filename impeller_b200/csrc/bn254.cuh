@@ -3,12 +3,14 @@
 // Field elements are 8 little-endian 32-bit limbs in Montgomery form with
 // R = 2^256, the layout of the reference's mont::Element
 // (core/src/common/mont/src/field.cuh:906-1204) and of its C ABI.
-// Multiplication is coarsely integrated operand scanning on the integer
-// multiply pipe: per row, one carry chain of mad.lo and one of mad.hi for
-// a*b[i], one mul for the reduction factor, and one lo and one hi chain for
-// m*N.  Because N < 2^254, the running value stays below 3N < 2^256 even for
-// inputs in [0, 2N), so nine words hold every intermediate and no carry ever
-// leaves word 8.
+// Multiplication is coarsely integrated operand scanning: per row of b, eight
+// 32x32->64 wide products of a*b[i] (one integer-multiply-pipe instruction
+// each) added in two carry chains on the ALU, the reduction factor m, and the
+// same for m*N.  Measured on B200 this mix (144 multiply-pipe + 272 ALU
+// instructions per product) beats separate mad.lo / mad.hi carry chains
+// (285 + 267), whose multiply pipe saturates first.  Because N < 2^254 the
+// running value stays below 3N < 2^256 even for inputs in [0, 2N), so nine
+// words hold every intermediate and no carry ever leaves word 8.
 //
 // Curve points use XYZZ coordinates (x = X/ZZ, y = Y/ZZZ, ZZ^3 = ZZZ^2), the
 // point representation of core/src/common/curve/src/curve_xyzz.cuh:252-418,
@@ -102,66 +104,50 @@ __device__ __forceinline__ void fe_reduce_once(Fe<F> &r, const u32 t[8]) {
     for (int i = 0; i < 8; i++) r.l[i] = bw ? t[i] : d[i];
 }
 
-// One CIOS row: t += a * bi; m = t0 * INV; t += m * N; t >>= 32.
-// t holds 9 words on entry (t[8] small) and on exit.
-#define BN_ROW(F, t, a, bi)                                                                              \
-    do {                                                                                                 \
-        u32 _m;                                                                                          \
-        asm("mad.lo.cc.u32  %0, %9,  %17, %0;\n\t"                                                       \
-            "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"                                                       \
-            "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"                                                       \
-            "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"                                                       \
-            "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"                                                       \
-            "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"                                                       \
-            "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"                                                       \
-            "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"                                                       \
-            "addc.u32       %8, %8, 0;\n\t"                                                              \
-            "mad.hi.cc.u32  %1, %9,  %17, %1;\n\t"                                                       \
-            "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"                                                       \
-            "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"                                                       \
-            "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"                                                       \
-            "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"                                                       \
-            "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"                                                       \
-            "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"                                                       \
-            "madc.hi.u32    %8, %16, %17, %8;"                                                           \
-            : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),     \
-              "+r"(t[7]), "+r"(t[8])                                                                     \
-            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),  \
-              "r"(bi));                                                                                  \
-        _m = t[0] * F::INV;                                                                              \
-        asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"                                                        \
-            "madc.lo.cc.u32 %1, %9, %11, %1;\n\t"                                                        \
-            "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"                                                        \
-            "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"                                                        \
-            "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"                                                        \
-            "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"                                                        \
-            "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"                                                        \
-            "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"                                                        \
-            "addc.u32       %8, %8, 0;\n\t"                                                              \
-            "mad.hi.cc.u32  %1, %9, %10, %1;\n\t"                                                        \
-            "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"                                                        \
-            "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"                                                        \
-            "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"                                                        \
-            "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"                                                        \
-            "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"                                                        \
-            "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"                                                        \
-            "madc.hi.u32    %8, %9, %17, %8;"                                                            \
-            : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),     \
-              "+r"(t[7]), "+r"(t[8])                                                                     \
-            : "r"(_m), "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5),         \
-              "n"(F::M6), "n"(F::M7));                                                                   \
-        t[0] = t[1]; t[1] = t[2]; t[2] = t[3]; t[3] = t[4];                                              \
-        t[4] = t[5]; t[5] = t[6]; t[6] = t[7]; t[7] = t[8]; t[8] = 0;                                    \
-    } while (0)
+// Even/odd row of wide products: t[0..8] += a * bi.  The eight 64-bit
+// products a_j * bi are formed with mul.wide; the even-j products tile words
+// 0..7 exactly (lo of a_j at word j, hi at j+1), the odd-j products tile words
+// 1..8, so one carry chain adds each tiling.  One multiply per 32x32 product
+// instead of a separate lo and hi multiply-add; the carries run on the
+// integer ALU.
+#define BN_EO_ROW(t, x0, x1, x2, x3, x4, x5, x6, x7, y)                                             \
+    asm("{\n\t.reg .u64 p0,p1,p2,p3,p4,p5,p6,p7;\n\t"                                                 \
+        ".reg .u32 l0,h0,l1,h1,l2,h2,l3,h3,l4,h4,l5,h5,l6,h6,l7,h7;\n\t"                               \
+        "mul.wide.u32 p0, %9, %17;\n\tmul.wide.u32 p1, %10, %17;\n\tmul.wide.u32 p2, %11, %17;\n\t"  \
+        "mul.wide.u32 p3, %12, %17;\n\tmul.wide.u32 p4, %13, %17;\n\tmul.wide.u32 p5, %14, %17;\n\t" \
+        "mul.wide.u32 p6, %15, %17;\n\tmul.wide.u32 p7, %16, %17;\n\t"                                \
+        "mov.b64 {l0,h0}, p0;\n\tmov.b64 {l1,h1}, p1;\n\tmov.b64 {l2,h2}, p2;\n\t"                   \
+        "mov.b64 {l3,h3}, p3;\n\tmov.b64 {l4,h4}, p4;\n\tmov.b64 {l5,h5}, p5;\n\t"                   \
+        "mov.b64 {l6,h6}, p6;\n\tmov.b64 {l7,h7}, p7;\n\t"                                            \
+        "add.cc.u32 %0, %0, l0;\n\taddc.cc.u32 %1, %1, h0;\n\taddc.cc.u32 %2, %2, l2;\n\t"           \
+        "addc.cc.u32 %3, %3, h2;\n\taddc.cc.u32 %4, %4, l4;\n\taddc.cc.u32 %5, %5, h4;\n\t"          \
+        "addc.cc.u32 %6, %6, l6;\n\taddc.cc.u32 %7, %7, h6;\n\taddc.u32 %8, %8, 0;\n\t"              \
+        "add.cc.u32 %1, %1, l1;\n\taddc.cc.u32 %2, %2, h1;\n\taddc.cc.u32 %3, %3, l3;\n\t"           \
+        "addc.cc.u32 %4, %4, h3;\n\taddc.cc.u32 %5, %5, l5;\n\taddc.cc.u32 %6, %6, h5;\n\t"          \
+        "addc.cc.u32 %7, %7, l7;\n\taddc.u32 %8, %8, h7;\n\t}"                                       \
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),       \
+          "+r"(t[7]), "+r"(t[8])                                                                     \
+        : x0, x1, x2, x3, x4, x5, x6, x7, "r"(y))
 
-// Montgomery product a*b*R^{-1} mod N, fully reduced (inputs reduced).
+// Montgomery product a*b*R^{-1} mod N, fully reduced (inputs reduced):
+// per row of b, the even/odd wide-product row for a*b[i], the reduction
+// factor m, the even/odd row for m*N, a one-word shift.
 template <class F>
 __device__ __forceinline__ Fe<F> fe_mul(const Fe<F> &a, const Fe<F> &b) {
     u32 t[9];
 #pragma unroll
     for (int i = 0; i < 9; i++) t[i] = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) BN_ROW(F, t, a.l, b.l[i]);
+    for (int i = 0; i < 8; i++) {
+        BN_EO_ROW(t, "r"(a.l[0]), "r"(a.l[1]), "r"(a.l[2]), "r"(a.l[3]), "r"(a.l[4]), "r"(a.l[5]), "r"(a.l[6]),
+                  "r"(a.l[7]), b.l[i]);
+        const u32 m = t[0] * F::INV;
+        BN_EO_ROW(t, "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5), "n"(F::M6),
+                  "n"(F::M7), m);
+#pragma unroll
+        for (int k = 0; k < 8; k++) t[k] = t[k + 1];
+        t[8] = 0;
+    }
     Fe<F> r;
     fe_reduce_once<F>(r, t);
     return r;
@@ -310,6 +296,105 @@ __device__ __forceinline__ Fe<F> fe_inv(const Fe<F> &a) {
     return fe_pow<F>(a, e);
 }
 
+// Single-thread-latency inversion for the few conversions to affine form at
+// the end of an MSM: binary extended Euclid on the integer representative
+// (Montgomery form a = A*R) gives a^{-1} = A^{-1} R^{-1}; one Montgomery
+// product with R^3 mod N turns it into A^{-1} R.  Variable time (the inputs
+// are public).  Inverse of zero is zero.  The loop is bounded: every step
+// shrinks u + v by at least one bit.
+template <class F>
+__device__ __forceinline__ bool u256_is_one(const u32 x[8]) {
+    return x[0] == 1 && (x[1] | x[2] | x[3] | x[4] | x[5] | x[6] | x[7]) == 0;
+}
+
+__device__ __forceinline__ void u256_shr1(u32 x[8], u32 top) {
+#pragma unroll
+    for (int i = 0; i < 7; i++) x[i] = __funnelshift_r(x[i], x[i + 1], 1);
+    x[7] = (x[7] >> 1) | (top << 31);
+}
+
+__device__ __forceinline__ bool u256_geq(const u32 a[8], const u32 b[8]) {
+    for (int i = 7; i >= 0; i--)
+        if (a[i] != b[i]) return a[i] > b[i];
+    return true;
+}
+
+__device__ __forceinline__ void u256_sub(u32 a[8], const u32 b[8]) {
+    asm("sub.cc.u32  %0, %0, %8;\n\t"
+        "subc.cc.u32 %1, %1, %9;\n\t"
+        "subc.cc.u32 %2, %2, %10;\n\t"
+        "subc.cc.u32 %3, %3, %11;\n\t"
+        "subc.cc.u32 %4, %4, %12;\n\t"
+        "subc.cc.u32 %5, %5, %13;\n\t"
+        "subc.cc.u32 %6, %6, %14;\n\t"
+        "subc.u32    %7, %7, %15;"
+        : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7])
+        : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+}
+
+// x = x / 2 mod N for x < N (N odd): if x is odd, (x + N) / 2.
+template <class F>
+__device__ __forceinline__ void fe_half(u32 x[8]) {
+    if (x[0] & 1u) {
+        u32 c;
+        asm("add.cc.u32  %0, %0, %9;\n\t"
+            "addc.cc.u32 %1, %1, %10;\n\t"
+            "addc.cc.u32 %2, %2, %11;\n\t"
+            "addc.cc.u32 %3, %3, %12;\n\t"
+            "addc.cc.u32 %4, %4, %13;\n\t"
+            "addc.cc.u32 %5, %5, %14;\n\t"
+            "addc.cc.u32 %6, %6, %15;\n\t"
+            "addc.cc.u32 %7, %7, %16;\n\t"
+            "addc.u32    %8, 0, 0;"
+            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]), "+r"(x[7]),
+              "=r"(c)
+            : "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5), "n"(F::M6), "n"(F::M7));
+        u256_shr1(x, c);
+    } else {
+        u256_shr1(x, 0);
+    }
+}
+
+template <class F>
+__device__ __noinline__ Fe<F> fe_inv_binary(const Fe<F> &a, const Fe<F> &r3) {
+    if (fe_is_zero(a)) return a;
+    u32 u[8], v[8];
+    Fe<F> x1 = fe_zero<F>(), x2 = fe_zero<F>();
+    x1.l[0] = 1;
+#pragma unroll
+    for (int i = 0; i < 8; i++) u[i] = a.l[i];
+    v[0] = F::M0; v[1] = F::M1; v[2] = F::M2; v[3] = F::M3;
+    v[4] = F::M4; v[5] = F::M5; v[6] = F::M6; v[7] = F::M7;
+    // One shift or one subtraction per step; a valid input (0 < a < N, N
+    // prime) needs at most ~4 * 254 steps.  The zero check and the step bound
+    // keep a non-canonical input from looping: it yields zero.
+    bool done = false;
+    for (int step = 0; step < 4096; step++) {
+        if (u256_is_one<F>(u) || u256_is_one<F>(v)) {
+            done = true;
+            break;
+        }
+        if ((u[0] | u[1] | u[2] | u[3] | u[4] | u[5] | u[6] | u[7]) == 0 ||
+            (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) == 0)
+            break;
+        if (!(u[0] & 1u)) {
+            u256_shr1(u, 0);
+            fe_half<F>(x1.l);
+        } else if (!(v[0] & 1u)) {
+            u256_shr1(v, 0);
+            fe_half<F>(x2.l);
+        } else if (u256_geq(u, v)) {
+            u256_sub(u, v);
+            x1 = fe_sub<F>(x1, x2);
+        } else {
+            u256_sub(v, u);
+            x2 = fe_sub<F>(x2, x1);
+        }
+    }
+    if (!done) return fe_zero<F>();
+    return fe_mul<F>(u256_is_one<F>(u) ? x1 : x2, r3);
+}
+
 template <class F>
 __device__ __forceinline__ Fe<F> fe_load(const u32 *p) {
     Fe<F> r;
@@ -453,6 +538,29 @@ __device__ __forceinline__ Xyzz xyzz_add(const Xyzz &p, const Xyzz &q) {
     Fq t = fe_mul(s1, ppp);
     r.x = fe_sub(fe_sub(fe_sub(fe_sqr(R), ppp), Q), Q);
     r.y = fe_sub(fe_mul(R, fe_sub(Q, r.x)), t);
+    return r;
+}
+
+__device__ __forceinline__ Fq fq_r3() {
+    Fq r;  // R^3 mod p
+    r.l[0] = 0xda1530dfu; r.l[1] = 0xb1cd6dafu; r.l[2] = 0xa7283db6u; r.l[3] = 0x62f210e6u;
+    r.l[4] = 0x0ada0afbu; r.l[5] = 0xef7f0b0cu; r.l[6] = 0x2d592544u; r.l[7] = 0x20fd6e90u;
+    return r;
+}
+
+// Canonical affine form; identity -> (0, 0).  Latency-optimised (binary
+// inversion): used once per MSM result.
+__device__ __forceinline__ Affine xyzz_to_affine_fast(const Xyzz &p) {
+    Affine r;
+    if (xyzz_is_identity(p)) {
+        r.x = fe_zero<FqP>();
+        r.y = fe_zero<FqP>();
+        return r;
+    }
+    Fq a = fe_inv_binary<FqP>(p.zzz, fq_r3());
+    Fq b = fe_sqr(fe_mul(p.zz, a));
+    r.x = fe_mul(p.x, b);
+    r.y = fe_mul(p.y, a);
     return r;
 }
 

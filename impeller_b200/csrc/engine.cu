@@ -128,9 +128,9 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
         const u32 nthreads = (w.nbuckets + w.chunk - 1) / w.chunk;
         const u32 nblocks = (nthreads + REDUCE_BLOCK - 1) / REDUCE_BLOCK;
         w.part_base = nparts;
-        w.nparts = nblocks;
+        w.nparts = nblocks * REDUCE_WARPS;  // one partial per reduce warp
         for (u32 k = 0; k < nblocks; k++) rblocks.push_back(make_uint2(wi, k));
-        nparts += nblocks;
+        nparts += w.nparts;
     }
     p.nparts = nparts;
     p.nwins = (u32)wins.size();
@@ -313,7 +313,7 @@ cudaError_t Plan::launch(void *scratch, const u32 *points, u32 *results, int car
     MARK(7);
 
     WindowSumArgs wa{d_desc, d_wins, parts, parts_s, nwins, wres};
-    k_window_sum<<<(nwins + 3) / 4, 128, 0, st>>>(wa);
+    k_window_sum<<<nwins, WSUM_BLOCK, 0, st>>>(wa);
     CK_LAUNCH("k_window_sum");
     FinalArgs fa2{d_desc, wres, M, carry_mode == 0 ? nullptr : carry, carry_mode == 2 ? 0 : 1, res};
     k_final<<<(M + 3) / 4, 128, 0, st>>>(fa2);
@@ -363,8 +363,21 @@ cudaError_t precompute_tables(u32 *d_points, u64 n, u32 shift, u32 n_tables, cud
 
 // ------------------------------------------------------------ window table
 
+struct WindowEntry {
+    u32 log2n, c, tables_c;  // best plain window; tables window (0: plain is faster)
+};
+
+static const WindowEntry k_default_table[] = {
+#include "autotune_default.inc"
+    {0u, 0u, 0u}};
+
 static std::mutex g_tab_mu;
-static std::vector<std::pair<u32, u32>> g_window_table;  // (log2 n, c)
+static std::vector<WindowEntry> g_window_table = [] {
+    std::vector<WindowEntry> t;
+    for (const WindowEntry &e : k_default_table)
+        if (e.c) t.push_back(e);
+    return t;
+}();
 
 // Cost model used when no measured table is loaded: W(c) windows of n
 // mixed additions (10 Fq products each) plus the bucket reduction of
@@ -384,32 +397,35 @@ static u32 model_window(u64 n) {
     return best;
 }
 
-// With resident window tables of window c_tab, an MSM of n points costs
-// W(c_tab) * n mixed additions plus one bucket set of 2^(c_tab-1); without,
-// the cost model's best plain window.  Pick the cheaper.
-u32 tables_worthwhile(u64 n, u32 c_tab) {
-    if (c_tab == 0) return 0;
-    const u32 c = default_window(n);
-    const double plain = (double)digit_windows(c) * ((double)n * 10.0 + std::ldexp(1.0, (int)c - 1) * 45.0);
-    const double tab = (double)digit_windows(c_tab) * (double)n * 10.0 + std::ldexp(1.0, (int)c_tab - 1) * 45.0;
-    return tab < plain ? c_tab : 0;
+static const WindowEntry *nearest_entry(u64 n) {
+    if (g_window_table.empty()) return nullptr;
+    const double lg = std::log2((double)n);
+    const WindowEntry *best = &g_window_table[0];
+    double bd = 1e300;
+    for (const WindowEntry &e : g_window_table) {
+        double dd = std::fabs(lg - (double)e.log2n);
+        if (dd < bd) {
+            bd = dd;
+            best = &e;
+        }
+    }
+    return best;
 }
 
 u32 default_window(u64 n) {
     if (n == 0) return 0;
     std::lock_guard<std::mutex> g(g_tab_mu);
-    if (g_window_table.empty()) return model_window(n);
-    const double lg = std::log2((double)n);
-    u32 best = g_window_table[0].second;
-    double bd = 1e300;
-    for (auto &e : g_window_table) {
-        double dd = std::fabs(lg - (double)e.first);
-        if (dd < bd) {
-            bd = dd;
-            best = e.second;
-        }
-    }
-    return best;
+    const WindowEntry *e = nearest_entry(n);
+    return e ? e->c : model_window(n);
+}
+
+// Window of the resident tables the table recommends for MSMs of n points
+// (0: plain windows are faster at that size).
+u32 table_window(u64 n) {
+    if (n == 0) return 0;
+    std::lock_guard<std::mutex> g(g_tab_mu);
+    const WindowEntry *e = nearest_entry(n);
+    return e ? e->tables_c : 0;
 }
 
 }  // namespace impeller
@@ -436,11 +452,10 @@ struct impeller_ctx {
     std::map<std::pair<u32, u32>, std::unique_ptr<Plan>> plans;
 };
 
+// With resident tables the context uses them for the sizes whose best
+// (measured) tables window is the one it holds; other sizes run plain.
 static u32 ctx_window(const impeller_ctx *ctx, u64 n) {
-    if (ctx->tables) {
-        u32 c = tables_worthwhile(n, ctx->table_c);
-        if (c) return c;
-    }
+    if (ctx->tables && table_window(n) == ctx->table_c) return ctx->table_c;
     return default_window(n);
 }
 
@@ -485,14 +500,18 @@ const char *impeller_version(void) { return "impeller-b200-msm 0.1 (sm_100a)"; }
 
 unsigned int impeller_default_window(uint64_t n) { return impeller::default_window(n); }
 
-cudaError_t impeller_set_window_table(const uint32_t *log2n, const uint32_t *c, uint32_t count) {
-    std::vector<std::pair<u32, u32>> t;
+unsigned int impeller_table_window(uint64_t n) { return impeller::table_window(n); }
+
+cudaError_t impeller_set_window_table(const uint32_t *log2n, const uint32_t *c, const uint32_t *tables_c,
+                                      uint32_t count) {
+    std::vector<WindowEntry> t;
     for (u32 i = 0; i < count; i++) {
-        if (c[i] < 3 || c[i] > 31) {
+        const u32 ct = tables_c ? tables_c[i] : 0;
+        if (c[i] < 3 || c[i] > 31 || (ct && (ct < 3 || ct > 31))) {
             set_error("window table entry outside [3, 31]");
             return cudaErrorInvalidValue;
         }
-        t.emplace_back(log2n[i], c[i]);
+        t.push_back(WindowEntry{log2n[i], c[i], ct});
     }
     std::lock_guard<std::mutex> g(g_tab_mu);
     g_window_table = t;

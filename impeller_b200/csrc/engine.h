@@ -26,6 +26,7 @@ struct MsmShape {
 
 u32 digit_windows(u32 c);  // ceil(254 / c)
 u32 default_window(u64 n);  // autotune table (or the cost model)
+u32 table_window(u64 n);    // tables window the autotune table recommends (0: none)
 
 // Device property cache.
 int sm_count(int device);

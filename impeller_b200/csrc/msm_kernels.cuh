@@ -99,21 +99,29 @@ struct DigitIter {
     }
 };
 
+// Lanes of a warp whose digits hit the same bucket share one atomic: heavy
+// buckets (the top window in a shared bucket set, the 0 / 1 / small scalars of
+// witness-like inputs) would otherwise serialize on a handful of addresses.
+// Every lane of the warp runs the same number of windows, so the match is
+// always taken with the full warp present.
 __global__ void k_histogram(const MsmDesc *__restrict__ descs, u32 *__restrict__ counts) {
     const MsmDesc d = descs[blockIdx.y];
     const u32 B = 1u << (d.c - 1);
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 stride = gridDim.x * blockDim.x;
+    for (u32 base = blockIdx.x * blockDim.x; base < d.n; base += stride) {
+        const u32 i = base + threadIdx.x;
+        const bool live = i < d.n;
         DigitIter it;
-        it.v = fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i));
+        it.v = live ? fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i)) : fe_zero<FrP>();
         it.c = d.c;
         it.carry = 0;
         for (u32 w = 0; w < d.n_logical; w++) {
             u32 mag, sign;
             it.next(w, d.n_logical, mag, sign);
-            if (mag) {
-                u32 pw = w % d.n_windows;
-                atomicAdd(&counts[d.bucket_base + pw * B + mag - 1], 1u);
-            }
+            const u32 key = mag ? d.bucket_base + (w % d.n_windows) * B + mag - 1 : NONE;
+            const u32 peers = __match_any_sync(0xffffffffu, key);
+            if (key != NONE && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (u32)__popc(peers));
         }
     }
 }
@@ -121,19 +129,28 @@ __global__ void k_histogram(const MsmDesc *__restrict__ descs, u32 *__restrict__
 __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ cursor, u32 *__restrict__ entries) {
     const MsmDesc d = descs[blockIdx.y];
     const u32 B = 1u << (d.c - 1);
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 stride = gridDim.x * blockDim.x;
+    for (u32 base = blockIdx.x * blockDim.x; base < d.n; base += stride) {
+        const u32 i = base + threadIdx.x;
+        const bool live = i < d.n;
         DigitIter it;
-        it.v = fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i));
+        it.v = live ? fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i)) : fe_zero<FrP>();
         it.c = d.c;
         it.carry = 0;
         for (u32 w = 0; w < d.n_logical; w++) {
             u32 mag, sign;
             it.next(w, d.n_logical, mag, sign);
-            if (mag) {
-                u32 pw = w % d.n_windows;
-                u32 table = w / d.n_windows;
-                u32 pos = atomicAdd(&cursor[d.bucket_base + pw * B + mag - 1], 1u);
-                entries[pos] = ((table * d.table_stride + i) << 1) | sign;
+            const u32 key = mag ? d.bucket_base + (w % d.n_windows) * B + mag - 1 : NONE;
+            const u32 peers = __match_any_sync(0xffffffffu, key);
+            const u32 leader = __ffs(peers) - 1;
+            u32 pos = 0;
+            if (key != NONE && lane == leader) pos = atomicAdd(&cursor[key], (u32)__popc(peers));
+            pos = __shfl_sync(0xffffffffu, pos, leader);
+            if (key != NONE) {
+                const u32 rank = __popc(peers & ((1u << lane) - 1u));
+                const u32 table = w / d.n_windows;
+                entries[pos + rank] = ((table * d.table_stride + i) << 1) | sign;
             }
         }
     }
@@ -357,24 +374,24 @@ __global__ void k_fixup_long(FixupArgs f) {
 
 // ----------------------------------------------------------------- reduce
 //
-// Window total T = sum_{k=1..B} k * S_k.  Thread j of a window owns the
-// weights (jL, (j+1)L] and forms by a running sum from the top
+// Window total T = sum_{k=1..B} k * S_k.  Lane j of a window owns the weights
+// (jL, (j+1)L] and forms by a running sum from the top
 //   sum_j = sum_k S_k   and   sos_j = sum_k (k - jL) * S_k.
 // Since sum_j j * sum_j = sum_{i>=1} suffix_i with suffix_i = sum_{j>=i} sum_j,
 //   T = sum_j (sos_j + L * suffix_{j+1}),
-// so each thread needs only the exclusive suffix of the chunk sums (a scan)
-// and log2(L) doublings -- no per-thread scalar multiplication.  Inside a
-// block of 128 threads the suffix is a warp shuffle scan; the part owed to
-// later blocks of the window is sum_b b * S_b over the block totals S_b,
-// scaled by 128 L, and is added by k_window_sum.
+// so each lane needs only the exclusive suffix of the chunk sums (a warp
+// shuffle scan) and log2(L) doublings -- no per-lane scalar multiplication.
+// Each warp leaves V_w = sum over its lanes of (sos_j + L * warp-local
+// suffix_{j+1}) and S_w = sum of its chunk sums; the part owed to later warps
+// of the window is 32 L * sum_w w * S_w, added by k_window_sum.
 
 struct ReduceArgs {
     const WinDesc *wins;
     const uint2 *blocks;  // (window, block-in-window) per reduce block
     const u32 *offsets;
     const u32 *buckets;
-    u32 *parts_v;         // XYZZ per reduce block: sum_j (sos_j + L * local suffix_{j+1})
-    u32 *parts_s;         // XYZZ per reduce block: block total of sum_j
+    u32 *parts_v;         // XYZZ per reduce warp
+    u32 *parts_s;         // XYZZ per reduce warp
 };
 
 static constexpr u32 REDUCE_BLOCK = 128;
@@ -383,8 +400,6 @@ static constexpr u32 REDUCE_WARPS = REDUCE_BLOCK / 32;
 __device__ __forceinline__ u32 ilog2(u32 x) { return 31 - __clz(x); }
 
 __global__ void __launch_bounds__(REDUCE_BLOCK) k_reduce(ReduceArgs r) {
-    __shared__ __align__(16) u32 sm_tot[REDUCE_WARPS][32];
-    __shared__ __align__(16) u32 sm_v[REDUCE_WARPS][32];
     const uint2 blk = r.blocks[blockIdx.x];
     const WinDesc wd = r.wins[blk.x];
     const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
@@ -406,29 +421,16 @@ __global__ void __launch_bounds__(REDUCE_BLOCK) k_reduce(ReduceArgs r) {
         Xyzz y = xyzz_shfl_down(x, o);
         if (lane + o < 32) x = xyzz_add(x, y);
     }
-    if (lane == 0) xyzz_store(&sm_tot[wid][0], x);
-    __syncthreads();
-    Xyzz later = xyzz_identity();  // totals of the later warps of this block
-    for (u32 w2 = wid + 1; w2 < REDUCE_WARPS; w2++) later = xyzz_add(later, xyzz_load(&sm_tot[w2][0]));
     Xyzz ex = xyzz_shfl_down(x, 1);
     if (lane == 31) ex = xyzz_identity();
-    ex = xyzz_add(ex, later);
-    const u32 lg = ilog2(wd.chunk);
-    for (u32 k = 0; k < lg; k++) ex = xyzz_dbl(ex);
+    for (u32 k = 0, lg = ilog2(wd.chunk); k < lg; k++) ex = xyzz_dbl(ex);
     Xyzz v = xyzz_add(sos, ex);
 #pragma unroll 1
     for (u32 o = 16; o; o >>= 1) v = xyzz_add(v, xyzz_shfl_down(v, o));
-    if (lane == 0) xyzz_store(&sm_v[wid][0], v);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        Xyzz acc = xyzz_load(&sm_v[0][0]);
-        Xyzz tot = xyzz_load(&sm_tot[0][0]);
-        for (u32 k = 1; k < REDUCE_WARPS; k++) {
-            acc = xyzz_add(acc, xyzz_load(&sm_v[k][0]));
-            tot = xyzz_add(tot, xyzz_load(&sm_tot[k][0]));
-        }
-        xyzz_store(r.parts_v + (size_t)(wd.part_base + blk.y) * 32, acc);
-        xyzz_store(r.parts_s + (size_t)(wd.part_base + blk.y) * 32, tot);
+    if (lane == 0) {
+        const size_t slot = (size_t)(wd.part_base + blk.y * REDUCE_WARPS + wid) * 32;
+        xyzz_store(r.parts_v + slot, v);
+        xyzz_store(r.parts_s + slot, x);
     }
 }
 
@@ -441,53 +443,87 @@ struct WindowSumArgs {
     u32 *wres;  // XYZZ per window: 2^(c * pw) * T
 };
 
-// One warp per window: T = sum_b V_b + 128 L * sum_b b * S_b, then weighted by
-// 2^(c * physical window) so the MSM result is the plain sum of its windows.
-__global__ void k_window_sum(WindowSumArgs a) {
-    const u32 lane = threadIdx.x & 31u;
-    const u32 win = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+static constexpr u32 WSUM_BLOCK = 256;
+static constexpr u32 WSUM_WARPS = WSUM_BLOCK / 32;
+
+// One block per window: T = sum_w V_w + 32 L * sum_w w * S_w (thread t owns a
+// group of g consecutive warp partials, a block-wide suffix scan gives the
+// cross-group weights), then weighted by 2^(c * physical window) so the MSM
+// result is the plain sum of its windows.
+__global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
+    __shared__ __align__(16) u32 sm_a[WSUM_WARPS][32];
+    __shared__ __align__(16) u32 sm_b[WSUM_WARPS][32];
+    const u32 win = blockIdx.x;
     if (win >= a.nwins) return;
+    const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     const WinDesc wd = a.wins[win];
     const MsmDesc d = a.descs[wd.msm];
-    const u32 pw = win - d.win_base;
-    // lane l owns a group of g block partials (g a power of two)
     u32 g = 1;
-    while (g * 32 < wd.nparts) g <<= 1;
-    const u32 b0 = lane * g;
-    // group-local weights: partial b carries weight b - b0, so the running
-    // sum adds into `sos` before each step down and not after the last one
-    Xyzz vsum = xyzz_identity(), ssum = xyzz_identity(), sos = xyzz_identity();
+    while (g * WSUM_BLOCK < wd.nparts) g <<= 1;
+    const u32 b0 = threadIdx.x * g;
     const u32 top = min(b0 + g, wd.nparts);
+    // group-local weights: partial b carries weight b - b0
+    Xyzz vsum = xyzz_identity(), ssum = xyzz_identity(), sos = xyzz_identity();
     for (u32 b = top; b > b0; b--) {
         const size_t slot = (size_t)(wd.part_base + b - 1) * 32;
-        if (b < top) sos = xyzz_add(sos, ssum);  // sum (b' - b0) * S_b' over the group
+        if (b < top) sos = xyzz_add(sos, ssum);
         vsum = xyzz_add(vsum, xyzz_load(a.parts_v + slot));
         ssum = xyzz_add(ssum, xyzz_load(a.parts_s + slot));
     }
-    // sum_b b * S_b = sum_l (sos_l + g * suffix_{l+1}) over lanes
+    // block-wide inclusive suffix of ssum: warp scan, then a scan of the warp totals
     Xyzz x = ssum;
 #pragma unroll 1
     for (u32 o = 1; o < 32; o <<= 1) {
         Xyzz y = xyzz_shfl_down(x, o);
         if (lane + o < 32) x = xyzz_add(x, y);
     }
+    if (lane == 0) xyzz_store(&sm_a[wid][0], x);
+    __syncthreads();
+    if (wid == 0) {
+        Xyzz t = lane < WSUM_WARPS ? xyzz_load(&sm_a[lane][0]) : xyzz_identity();
+#pragma unroll 1
+        for (u32 o = 1; o < WSUM_WARPS; o <<= 1) {
+            Xyzz y = xyzz_shfl_down(t, o);
+            if (lane + o < WSUM_WARPS) t = xyzz_add(t, y);
+        }
+        if (lane < WSUM_WARPS) xyzz_store(&sm_b[lane][0], t);  // suffix over warps >= lane
+    }
+    __syncthreads();
+    Xyzz later = wid + 1 < WSUM_WARPS ? xyzz_load(&sm_b[wid + 1][0]) : xyzz_identity();
     Xyzz ex = xyzz_shfl_down(x, 1);
     if (lane == 31) ex = xyzz_identity();
+    ex = xyzz_add(ex, later);
     for (u32 k = 0, lg = ilog2(g); k < lg; k++) ex = xyzz_dbl(ex);
-    Xyzz rs = xyzz_add(sos, ex);
+    Xyzz rs = xyzz_add(sos, ex);  // this group's share of sum_w w * S_w
 #pragma unroll 1
     for (u32 o = 16; o; o >>= 1) {
         rs = xyzz_add(rs, xyzz_shfl_down(rs, o));
         vsum = xyzz_add(vsum, xyzz_shfl_down(vsum, o));
     }
+    __syncthreads();
     if (lane == 0) {
-        const u32 shift = ilog2(wd.chunk) + ilog2(REDUCE_BLOCK);
-        for (u32 k = 0; k < shift; k++) rs = xyzz_dbl(rs);
-        Xyzz t = xyzz_add(vsum, rs);
-        const u32 dbls = d.c * pw;
-        if (!xyzz_is_identity(t))
-            for (u32 k = 0; k < dbls; k++) t = xyzz_dbl(t);
-        xyzz_store(a.wres + (size_t)win * 32, t);
+        xyzz_store(&sm_a[wid][0], rs);
+        xyzz_store(&sm_b[wid][0], vsum);
+    }
+    __syncthreads();
+    if (wid == 0) {
+        Xyzz r2 = lane < WSUM_WARPS ? xyzz_load(&sm_a[lane][0]) : xyzz_identity();
+        Xyzz v2 = lane < WSUM_WARPS ? xyzz_load(&sm_b[lane][0]) : xyzz_identity();
+#pragma unroll 1
+        for (u32 o = WSUM_WARPS / 2; o; o >>= 1) {
+            r2 = xyzz_add(r2, xyzz_shfl_down(r2, o));
+            v2 = xyzz_add(v2, xyzz_shfl_down(v2, o));
+        }
+        if (lane == 0) {
+            const u32 shift = ilog2(wd.chunk) + 5;  // 32 lanes per warp partial
+            for (u32 k = 0; k < shift; k++) r2 = xyzz_dbl(r2);
+            Xyzz t = xyzz_add(v2, r2);
+            const u32 pw = win - d.win_base;
+            const u32 dbls = d.c * pw;
+            if (!xyzz_is_identity(t))
+                for (u32 k = 0; k < dbls; k++) t = xyzz_dbl(t);
+            xyzz_store(a.wres + (size_t)win * 32, t);
+        }
     }
 }
 
@@ -513,7 +549,7 @@ __global__ void k_final(FinalArgs f) {
     if (lane != 0) return;
     if (f.carry) acc = xyzz_add(acc, xyzz_load(f.carry + (size_t)m * 32));
     if (f.emit_affine) {
-        Affine r = xyzz_to_affine(acc);
+        Affine r = xyzz_to_affine_fast(acc);
         affine_store(f.results + (size_t)m * 16, r);
     } else {
         xyzz_store(f.carry + (size_t)m * 32, acc);
@@ -525,7 +561,7 @@ __global__ void k_combine(const u32 *xyzz, u32 k, u32 *out) {
     if (blockIdx.x || threadIdx.x) return;
     Xyzz acc = xyzz_identity();
     for (u32 i = 0; i < k; i++) acc = xyzz_add(acc, xyzz_load(xyzz + (size_t)i * 32));
-    affine_store(out, xyzz_to_affine(acc));
+    affine_store(out, xyzz_to_affine_fast(acc));
 }
 
 }  // namespace impeller

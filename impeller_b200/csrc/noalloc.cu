@@ -64,13 +64,15 @@ constexpr u32 E_MAX = W * MAX_N;                       // entries
 constexpr u32 ACC_BLOCKS = 64, ACC_THREADS = 256, T = ACC_BLOCKS * ACC_THREADS;
 constexpr u32 CHUNK = 16;                              // buckets per reduce thread
 constexpr u32 RBLOCKS_PER_WIN = (B / CHUNK + K::REDUCE_BLOCK - 1) / K::REDUCE_BLOCK;
-constexpr u32 NPARTS = W * RBLOCKS_PER_WIN;
+constexpr u32 NPARTS_PER_WIN = RBLOCKS_PER_WIN * K::REDUCE_WARPS;
+constexpr u32 NPARTS = W * NPARTS_PER_WIN;
+constexpr u32 NRBLOCKS = W * RBLOCKS_PER_WIN;
 
 constexpr size_t up(size_t x) { return (x + 255) / 256 * 256; }
 constexpr size_t O_DESC = 0;
 constexpr size_t O_WINS = O_DESC + up(sizeof(MsmDesc));
 constexpr size_t O_RBLK = O_WINS + up(sizeof(WinDesc) * W);
-constexpr size_t O_COUNTS = O_RBLK + up(sizeof(uint2) * NPARTS);
+constexpr size_t O_COUNTS = O_RBLK + up(sizeof(uint2) * NRBLOCKS);
 constexpr size_t O_CURSOR = O_COUNTS + up((size_t)NB_PAD * 4);
 constexpr size_t O_OFFSETS = O_CURSOR + up((size_t)NB * 4);
 constexpr size_t O_TILES = O_OFFSETS + up((size_t)(NB + 1) * 4);
@@ -131,14 +133,14 @@ __global__ void k_noalloc_tables(unsigned char *base, const u32 *scalars, u32 n)
         x.bucket_base = i * B;
         x.nbuckets = B;
         x.chunk = CHUNK;
-        x.part_base = i * RBLOCKS_PER_WIN;
-        x.nparts = RBLOCKS_PER_WIN;
+        x.part_base = i * NPARTS_PER_WIN;
+        x.nparts = NPARTS_PER_WIN;
         x.msm = 0;
         x.pad0 = 0;
         x.pad1 = 0;
         w[i] = x;
     }
-    for (u32 i = t; i < NPARTS; i += blockDim.x) rb[i] = make_uint2(i / RBLOCKS_PER_WIN, i % RBLOCKS_PER_WIN);
+    for (u32 i = t; i < NRBLOCKS; i += blockDim.x) rb[i] = make_uint2(i / RBLOCKS_PER_WIN, i % RBLOCKS_PER_WIN);
 }
 
 cudaError_t fail(cudaError_t e, const char *what) {
@@ -217,10 +219,10 @@ extern "C" cudaError_t impeller_msm_device_noalloc(const uint32_t *d_points, con
     K::k_fixup_long<<<64, 256, 0, stream>>>(fa);
     NA_LAUNCHED("k_fixup_long");
     ReduceArgs ra{wins, rblk, offsets, buckets, parts_v, parts_s};
-    K::k_reduce<<<NPARTS, K::REDUCE_BLOCK, 0, stream>>>(ra);
+    K::k_reduce<<<NRBLOCKS, K::REDUCE_BLOCK, 0, stream>>>(ra);
     NA_LAUNCHED("k_reduce");
     WindowSumArgs wa{desc, wins, parts_v, parts_s, W, wres};
-    K::k_window_sum<<<(W + 3) / 4, 128, 0, stream>>>(wa);
+    K::k_window_sum<<<W, K::WSUM_BLOCK, 0, stream>>>(wa);
     NA_LAUNCHED("k_window_sum");
     FinalArgs fin{desc, wres, 1, nullptr, 1, d_result};
     K::k_final<<<1, 128, 0, stream>>>(fin);

@@ -279,15 +279,30 @@ def gen_scalars_device(n: int, seed: int = 0, stream_id: int = 1, dist: int = 0,
 
 
 def set_window_table(table: dict) -> None:
-    """Load an autotune table {log2 n: c} into the library."""
+    """Load an autotune table {log2 n: c or (c, tables_c)} into the library;
+    an empty dict selects the built-in cost model."""
     keys = sorted(table)
-    lg = (ctypes.c_uint32 * len(keys))(*keys)
-    cs = (ctypes.c_uint32 * len(keys))(*[int(table[k]) for k in keys])
-    _lib.check(_lib.load().impeller_set_window_table(lg, cs, len(keys)), "impeller_set_window_table")
+    cnt = len(keys)
+    vals = [table[k] if isinstance(table[k], tuple) else (table[k], 0) for k in keys]
+    lg = (ctypes.c_uint32 * cnt)(*keys)
+    cs = (ctypes.c_uint32 * cnt)(*[int(v[0]) for v in vals])
+    ct = (ctypes.c_uint32 * cnt)(*[int(v[1]) for v in vals])
+    _lib.check(_lib.load().impeller_set_window_table(lg, cs, ct, cnt), "impeller_set_window_table")
+
+
+def restore_default_window_table() -> None:
+    """Reinstall the measured table compiled into the library."""
+    from . import autotune
+    if not autotune.load_table():
+        set_window_table({})
 
 
 def default_window(n: int) -> int:
     return int(_lib.load().impeller_default_window(n))
+
+
+def table_window(n: int) -> int:
+    return int(_lib.load().impeller_table_window(n))
 
 
 # --------------------------------------------------- resident-SRS context

@@ -96,10 +96,17 @@ cudaError_t impeller_ctx_precompute(impeller_ctx *ctx, unsigned int c);
 /* Window an MSM of n points uses on this context when c == 0 is passed. */
 unsigned int impeller_ctx_window(const impeller_ctx *ctx, uint64_t n);
 
-/* Window size the autotune table picks for an MSM of n points (0 -> none). */
+/* Window size the autotune table picks for a plain MSM of n points. */
 unsigned int impeller_default_window(uint64_t n);
-/* Load an autotune table: `count` pairs (log2 n, c); nearest log2 n wins. */
-cudaError_t impeller_set_window_table(const uint32_t *log2n, const uint32_t *c, uint32_t count);
+/* Window of resident tables the autotune table recommends for MSMs of n
+ * points (0: the plain path is faster at that size). */
+unsigned int impeller_table_window(uint64_t n);
+/* Replace the autotune table (the library starts with the table measured by
+ * impeller_b200/autotune.py and compiled in): `count` entries (log2 n, plain
+ * window c, tables window or 0); the entry with the nearest log2 n applies.
+ * tables_c may be NULL.  count == 0 falls back to the built-in cost model. */
+cudaError_t impeller_set_window_table(const uint32_t *log2n, const uint32_t *c, const uint32_t *tables_c,
+                                      uint32_t count);
 
 /* One MSM over the first n resident points.  d_scalars: device, n x 8
  * uint32 (Montgomery Fr); d_result: device, 16 uint32.  c == 0 picks the
@@ -146,7 +153,7 @@ cudaError_t impeller_gen_points(uint32_t *d_out, uint64_t n, uint64_t seed, uint
 
 /* Element-wise field / point operations on the device, for parity tests.
  * field: 0 = Fq, 1 = Fr.  op: 0 add, 1 sub, 2 mul, 3 sqr, 4 neg, 5 to_mont,
- * 6 from_mont, 7 inv, 8 pow.  Point ops (affine in/out): 0 add (madd path),
+ * 6 from_mont, 7 inv (Fermat), 8 pow, 9 inv (binary extended Euclid).  Point ops (affine in/out): 0 add (madd path),
  * 1 dbl, 2 add via XYZZ+XYZZ, 3 k*P (k plain 256-bit). */
 cudaError_t impeller_test_field_op(int field, int op, const uint32_t *d_a, const uint32_t *d_b, uint32_t *d_out,
                                    uint64_t count, cudaStream_t s);

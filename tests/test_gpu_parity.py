@@ -74,6 +74,7 @@ def test_field_ops_match_oracle(M, field, modulus):
         assert (got == want).all(), (field, op)
     want = O.field_op(field, O.INV, a[:64])
     assert (field_op_gpu(M, field, O.INV, a[:64]) == want).all()
+    assert (field_op_gpu(M, field, 9, a[:64]) == want).all()  # binary extended Euclid
     want = O.field_op(field, O.POW, a[:32], b[:32])
     assert (field_op_gpu(M, field, O.POW, a[:32], b[:32]) == want).all()
 

@@ -61,10 +61,13 @@ def test_shim_has_reference_name_and_symbols(L):
 
 
 def test_window_table_roundtrip(L):
-    M.set_window_table({10: 7, 16: 12, 22: 17})
+    M.set_window_table({10: 7, 16: 12, 22: (17, 20)})
     assert M.default_window(1 << 16) == 12
     assert M.default_window(3 << 20) == 17  # nearest log2
-    M.set_window_table({})  # back to the cost model
+    assert M.table_window(1 << 22) == 20 and M.table_window(1 << 10) == 0
+    M.set_window_table({})  # the cost model
+    assert 3 <= M.default_window(1 << 20) <= 22 and M.table_window(1 << 20) == 0
+    M.restore_default_window_table()
 
 
 def test_missing_library_fails_loudly(tmp_path):
