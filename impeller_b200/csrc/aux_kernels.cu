@@ -170,27 +170,32 @@ __global__ void k_test_point(int op, const u32 *p, const u32 *q, u32 *out, u64 c
     affine_store(out + 16 * i, xyzz_to_affine(r));
 }
 
-// 16 independent accumulators per thread: 8 mad.lo and 8 mad.hi per step.
+// Peak of the 32x32 -> 64-bit multiply (mul.wide.u32) the Montgomery product
+// is built from: 16 independent products per thread per step, folded into
+// accumulators with xor so that no carry arithmetic competes for issue.
 __global__ void k_imad_peak(u32 *out, u32 iters, u32 seed) {
-    u32 a[8], lo[8], hi[8];
+    u32 a[8];
+    u64 acc[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         a[k] = seed * (threadIdx.x + 3 * k + 1) + blockIdx.x;
-        lo[k] = a[k] ^ 0x5bd1e995u;
-        hi[k] = a[k] + 0x9e3779b9u;
+        acc[k] = a[k];
     }
 #pragma unroll 1
     for (u32 it = 0; it < iters; it++) {
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-            asm volatile("mad.lo.u32 %0, %1, %2, %0;" : "+r"(lo[k]) : "r"(a[k]), "r"(a[(k + 1) & 7]));
-            asm volatile("mad.hi.u32 %0, %1, %2, %0;" : "+r"(hi[k]) : "r"(a[k]), "r"(a[(k + 3) & 7]));
+            u64 p, q;
+            asm volatile("mul.wide.u32 %0, %1, %2;" : "=l"(p) : "r"(a[k]), "r"(a[(k + 1) & 7]));
+            asm volatile("mul.wide.u32 %0, %1, %2;" : "=l"(q) : "r"(a[k]), "r"(a[(k + 3) & 7]));
+            acc[k] ^= p ^ q;
+            a[k] += (u32)it;
         }
     }
-    u32 x = 0;
+    u64 x = 0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) x ^= lo[k] ^ hi[k];
-    if (x == 0x12345678u) out[blockIdx.x * blockDim.x + threadIdx.x] = x;
+    for (int k = 0; k < 8; k++) x ^= acc[k];
+    if (x == 0x12345678ull) out[blockIdx.x * blockDim.x + threadIdx.x] = (u32)x;
 }
 
 // Dependent chains of one operation on one thread (op 0 Fq product,

@@ -747,6 +747,24 @@ cudaError_t impeller_batch_destroy(impeller_batch *b) {
 
 uint32_t impeller_batch_launches(const impeller_batch *b) { return b ? b->plan.launches() : 0; }
 
+cudaError_t impeller_batch_profile(impeller_batch *b, int enable) {
+    if (!b || (enable && b->graph)) {
+        set_error("impeller_batch_profile: needs a batch created without IMPELLER_BATCH_GRAPH");
+        return cudaErrorInvalidValue;
+    }
+    b->plan.set_profiling(enable != 0);
+    return cudaSuccess;
+}
+
+cudaError_t impeller_batch_profile_read(impeller_batch *b, double *ms_per_phase, uint32_t nphase, uint32_t *runs) {
+    if (!b || !ms_per_phase || nphase < (u32)Plan::NPHASE) {
+        set_error("impeller_batch_profile_read: need room for every phase");
+        return cudaErrorInvalidValue;
+    }
+    for (u32 i = 0; i < nphase; i++) ms_per_phase[i] = 0;
+    return b->plan.read_profile(ms_per_phase, runs);
+}
+
 cudaError_t impeller_batch_run(impeller_batch *b, const uint32_t *const *d_scalars, uint32_t *d_results,
                                cudaStream_t stream) {
     if (!b || !d_scalars || !d_results) {

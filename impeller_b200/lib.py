@@ -48,6 +48,9 @@ SIGNATURES: dict[str, tuple] = {
     "impeller_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "impeller_batch_run": (ctypes.c_int, [ctypes.c_void_p, c_void_pp, ctypes.c_void_p, ctypes.c_void_p]),
     "impeller_batch_launches": (ctypes.c_uint32, [ctypes.c_void_p]),
+    "impeller_batch_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "impeller_batch_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_uint32,
+                                                   ctypes.POINTER(ctypes.c_uint32)]),
     "impeller_gen_scalars": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                             ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
     "impeller_gen_points": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,

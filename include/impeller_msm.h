@@ -142,6 +142,10 @@ cudaError_t impeller_batch_run(impeller_batch *b, const uint32_t *const *d_scala
                                cudaStream_t stream);
 /* Kernel launches one run of the batch issues (for launch accounting). */
 uint32_t impeller_batch_launches(const impeller_batch *b);
+/* Per-phase timing of a batch created without IMPELLER_BATCH_GRAPH (same
+ * phases and semantics as impeller_ctx_profile / impeller_ctx_profile_read). */
+cudaError_t impeller_batch_profile(impeller_batch *b, int enable);
+cudaError_t impeller_batch_profile_read(impeller_batch *b, double *ms_per_phase, uint32_t nphase, uint32_t *runs);
 
 /* ------------------------------------------------------------------------
  * Seeded synthetic inputs, computed on the device (definitions shared with
@@ -160,9 +164,9 @@ cudaError_t impeller_test_field_op(int field, int op, const uint32_t *d_a, const
 cudaError_t impeller_test_point_op(int op, const uint32_t *d_p, const uint32_t *d_q, uint32_t *d_out,
                                    uint64_t count, cudaStream_t s);
 
-/* Integer multiply-add peak of `device`, measured: independent mad.lo /
- * mad.hi chains (the instruction mix of the Montgomery product), in 10^9
- * multiply-add instructions per second.  Blocks until done. */
+/* 32x32 -> 64-bit integer multiply peak of `device`, measured: independent
+ * mul.wide.u32 products (the products the Montgomery multiplication is built
+ * from), in 10^9 products per second.  Blocks until done. */
 cudaError_t impeller_imad_peak(int device, double *gops);
 
 /* Single-thread latency, in SM clock cycles, of a dependent chain of one
