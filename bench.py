@@ -380,6 +380,8 @@ def batched_vs_per_call(M, ctx, dev, args) -> dict:
     import torch
     rng = np.random.default_rng(0)
     sizes = [int(round(2 ** rng.uniform(10, 20))) for _ in range(64)]
+    for ct in sorted({M.table_window(s) for s in sizes} - {0}):
+        ctx.precompute(ct)  # every table set the batch's sizes use (resident next to the SRS)
     scal = [M.gen_scalars_device(s, seed=0, stream_id=1000 + i, device=dev) for i, s in enumerate(sizes)]
     total = sum(sizes)
     b = ctx.batch(sizes, graph=True)

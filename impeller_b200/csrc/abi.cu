@@ -71,7 +71,7 @@ struct CardLayout {
 };
 
 std::vector<MsmShape> group_shapes(const Config &cfg, u32 M, u32 n, u32 part_len) {
-    std::vector<MsmShape> s(M, MsmShape{n, cfg.c, cfg.n_windows, part_len});
+    std::vector<MsmShape> s(M, MsmShape{n, cfg.c, cfg.n_windows, part_len, 0});
     return s;
 }
 

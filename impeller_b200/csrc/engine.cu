@@ -77,7 +77,7 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
         const u32 nw = (s.n_windows == 0 || s.n_windows > W) ? W : s.n_windows;
         const u32 n_tables = (W + nw - 1) / nw;
         const u64 B = 1ull << (s.c - 1);
-        const u64 vmax = (u64)(n_tables - 1) * s.table_stride + s.n;
+        const u64 vmax = (u64)s.table_base + (u64)(n_tables - 1) * s.table_stride + s.n;
         if (n_tables > 1 && s.table_stride < s.n) {
             set_error("table stride smaller than the MSM size");
             return false;
@@ -95,7 +95,7 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
         d.table_stride = s.table_stride;
         d.bucket_base = (u32)nb;
         d.win_base = (u32)wins.size();
-        d.pad = 0;
+        d.table_base = s.table_base;
         for (u32 pw = 0; pw < nw; pw++) {
             WinDesc w{};
             w.bucket_base = (u32)(nb + pw * B);
@@ -316,7 +316,7 @@ cudaError_t Plan::launch(void *scratch, const u32 *points, u32 *results, int car
     k_window_sum<<<nwins, WSUM_BLOCK, 0, st>>>(wa);
     CK_LAUNCH("k_window_sum");
     FinalArgs fa2{d_desc, wres, M, carry_mode == 0 ? nullptr : carry, carry_mode == 2 ? 0 : 1, res};
-    k_final<<<(M + 3) / 4, 128, 0, st>>>(fa2);
+    k_final<<<(M + 31) / 32, 32, 0, st>>>(fa2);
     CK_LAUNCH("k_final");
     MARK(8);
 #undef MARK
@@ -447,15 +447,26 @@ struct impeller_ctx {
     u32 *d_result = nullptr;
     cudaEvent_t done = nullptr;  // last run that used the scratch
     bool profiling = false;
-    u32 *tables = nullptr;       // W(table_c) window tables, table j = 2^(j*c) * P
-    u32 table_c = 0;
+    // Resident window tables: one allocation holding the points (region 0)
+    // followed by table sets; set for window c has W(c) tables of len points,
+    // table j = 2^(j*c) * P, starting at point index base.
+    u32 *tables = nullptr;
+    u64 tables_points = 0;  // points held by `tables`
+    std::vector<std::pair<u32, u32>> sets;  // (c, base)
     std::map<std::pair<u32, u32>, std::unique_ptr<Plan>> plans;
 };
 
+static u32 ctx_set_base(const impeller_ctx *ctx, u32 c) {
+    for (auto &s : ctx->sets)
+        if (s.first == c) return s.second;
+    return NONE;
+}
+
 // With resident tables the context uses them for the sizes whose best
-// (measured) tables window is the one it holds; other sizes run plain.
+// (measured) tables window is one of the sets it holds; other sizes run plain.
 static u32 ctx_window(const impeller_ctx *ctx, u64 n) {
-    if (ctx->tables && table_window(n) == ctx->table_c) return ctx->table_c;
+    const u32 ct = table_window(n);
+    if (ct && ctx_set_base(ctx, ct) != NONE) return ct;
     return default_window(n);
 }
 
@@ -471,11 +482,12 @@ static cudaError_t ctx_reserve(impeller_ctx *ctx, size_t bytes, cudaStream_t st)
     return cudaSuccess;
 }
 
-// Shape of an MSM of n points with window c on this context: with resident
-// window tables for c every digit window shares one bucket set.
+// Shape of an MSM of n points with window c on this context: with a resident
+// table set for c every digit window shares one bucket set.
 static MsmShape ctx_shape(const impeller_ctx *ctx, u32 n, u32 c) {
-    if (ctx->tables && c == ctx->table_c) return MsmShape{n, c, 1, (u32)ctx->len};
-    return MsmShape{n, c, 0, 0};
+    const u32 base = ctx_set_base(ctx, c);
+    if (base != NONE) return MsmShape{n, c, 1, (u32)ctx->len, base};
+    return MsmShape{n, c, 0, 0, 0};
 }
 
 static const u32 *ctx_point_base(const impeller_ctx *ctx) { return ctx->tables ? ctx->tables : ctx->points; }
@@ -575,29 +587,34 @@ cudaError_t impeller_ctx_precompute(impeller_ctx *ctx, unsigned int c) {
         return cudaErrorInvalidValue;
     }
     std::lock_guard<std::mutex> g(ctx->mu);
+    if (ctx_set_base(ctx, c) != NONE) return cudaSuccess;
     CK(cudaSetDevice(ctx->device));
     CK(cudaDeviceSynchronize());
     const u32 W = digit_windows(c);
-    if ((u64)W * ctx->len >= (1ull << 31)) {
-        set_error("impeller_ctx_precompute: window tables exceed 2^31 points");
+    const u64 have = ctx->tables ? ctx->tables_points : ctx->len;  // region 0 = the points
+    const u64 total = have + (u64)W * ctx->len;
+    if (total >= (1ull << 31)) {
+        set_error("impeller_ctx_precompute: points and window tables exceed 2^31 points");
         return cudaErrorInvalidValue;
     }
-    if (ctx->tables) CK(cudaFree(ctx->tables));
-    ctx->tables = nullptr;
-    ctx->table_c = 0;
-    ctx->plans.clear();
     u32 *t = nullptr;
-    CK(cudaMalloc(&t, (size_t)W * std::max<u64>(ctx->len, 1) * 64));
-    cudaError_t e = cudaMemcpy(t, ctx->points, ctx->len * 64, cudaMemcpyDeviceToDevice);
-    if (e == cudaSuccess) e = precompute_tables(t, ctx->len, c, W, 0);
+    CK(cudaMalloc(&t, (size_t)std::max<u64>(total, 1) * 64));
+    const u32 *src = ctx->tables ? ctx->tables : ctx->points;
+    cudaError_t e = cudaMemcpy(t, src, have * 64, cudaMemcpyDeviceToDevice);
+    u32 *set = t + (size_t)have * 16;
+    if (e == cudaSuccess) e = cudaMemcpy(set, ctx->points, ctx->len * 64, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = precompute_tables(set, ctx->len, c, W, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         cudaFree(t);
         set_error(std::string("impeller_ctx_precompute: ") + cudaGetErrorString(e));
         return e;
     }
+    if (ctx->tables) cudaFree(ctx->tables);
     ctx->tables = t;
-    ctx->table_c = c;
+    ctx->tables_points = total;
+    ctx->sets.emplace_back(c, (u32)have);
+    ctx->plans.clear();
     return cudaSuccess;
 }
 

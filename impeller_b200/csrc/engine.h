@@ -22,6 +22,7 @@ struct MsmShape {
     u32 c;             // window bits
     u32 n_windows;     // bucket sets (physical windows); 0 -> one per digit window
     u32 table_stride;  // points per window table (used when n_windows < digit windows)
+    u32 table_base;    // point index of this MSM's table 0
 };
 
 u32 digit_windows(u32 c);  // ceil(254 / c)
@@ -40,7 +41,7 @@ struct PlanLayout {
 
 class Plan {
   public:
-    // Every MSM reads points[(w / n_windows) * table_stride + i].
+    // Every MSM reads points[table_base + (w / n_windows) * table_stride + i].
     static bool build(Plan &p, int device, const std::vector<MsmShape> &shapes);
     ~Plan();
 

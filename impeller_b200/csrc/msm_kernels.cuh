@@ -40,8 +40,9 @@ static constexpr u32 SCAN_PER_THREAD = 16;
 static constexpr u32 SCAN_TILE = SCAN_BLOCK * SCAN_PER_THREAD;
 
 // One MSM of a batch.  Virtual point index of digit window w of scalar i is
-// (w / n_windows) * table_stride + i: window tables hold 2^(j*n_windows*c)*P
-// (core/src/msm/src/msm.cuh:53-70 for the window / table relation).
+// table_base + (w / n_windows) * table_stride + i: window tables hold
+// 2^(j*n_windows*c)*P (core/src/msm/src/msm.cuh:53-70 for the window / table
+// relation); table_base selects one of several table sets kept in one array.
 struct MsmDesc {
     const u32 *scalars;  // n x 8 u32, Montgomery Fr
     u32 n;
@@ -51,7 +52,7 @@ struct MsmDesc {
     u32 table_stride;    // points per window table
     u32 bucket_base;     // global index of bucket (window 0, weight 1)
     u32 win_base;        // global index of physical window 0
-    u32 pad;
+    u32 table_base;      // index of this MSM's table 0 in the point array
 };
 
 // One physical window of one MSM (bucket reduction unit).
@@ -150,7 +151,7 @@ __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ c
             if (key != NONE) {
                 const u32 rank = __popc(peers & ((1u << lane) - 1u));
                 const u32 table = w / d.n_windows;
-                entries[pos + rank] = ((table * d.table_stride + i) << 1) | sign;
+                entries[pos + rank] = ((d.table_base + table * d.table_stride + i) << 1) | sign;
             }
         }
     }
@@ -399,7 +400,7 @@ static constexpr u32 REDUCE_WARPS = REDUCE_BLOCK / 32;
 
 __device__ __forceinline__ u32 ilog2(u32 x) { return 31 - __clz(x); }
 
-__global__ void __launch_bounds__(REDUCE_BLOCK) k_reduce(ReduceArgs r) {
+__global__ void __launch_bounds__(REDUCE_BLOCK, 3) k_reduce(ReduceArgs r) {
     const uint2 blk = r.blocks[blockIdx.x];
     const WinDesc wd = r.wins[blk.x];
     const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
@@ -440,7 +441,7 @@ struct WindowSumArgs {
     const u32 *parts_v;
     const u32 *parts_s;
     u32 nwins;
-    u32 *wres;  // XYZZ per window: 2^(c * pw) * T
+    u32 *wres;  // XYZZ per window: the window total T
 };
 
 static constexpr u32 WSUM_BLOCK = 256;
@@ -448,8 +449,7 @@ static constexpr u32 WSUM_WARPS = WSUM_BLOCK / 32;
 
 // One block per window: T = sum_w V_w + 32 L * sum_w w * S_w (thread t owns a
 // group of g consecutive warp partials, a block-wide suffix scan gives the
-// cross-group weights), then weighted by 2^(c * physical window) so the MSM
-// result is the plain sum of its windows.
+// cross-group weights).  k_final weights the windows by 2^(c * window).
 __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
     __shared__ __align__(16) u32 sm_a[WSUM_WARPS][32];
     __shared__ __align__(16) u32 sm_b[WSUM_WARPS][32];
@@ -457,7 +457,6 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
     if (win >= a.nwins) return;
     const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     const WinDesc wd = a.wins[win];
-    const MsmDesc d = a.descs[wd.msm];
     u32 g = 1;
     while (g * WSUM_BLOCK < wd.nparts) g <<= 1;
     const u32 b0 = threadIdx.x * g;
@@ -517,12 +516,7 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
         if (lane == 0) {
             const u32 shift = ilog2(wd.chunk) + 5;  // 32 lanes per warp partial
             for (u32 k = 0; k < shift; k++) r2 = xyzz_dbl(r2);
-            Xyzz t = xyzz_add(v2, r2);
-            const u32 pw = win - d.win_base;
-            const u32 dbls = d.c * pw;
-            if (!xyzz_is_identity(t))
-                for (u32 k = 0; k < dbls; k++) t = xyzz_dbl(t);
-            xyzz_store(a.wres + (size_t)win * 32, t);
+            xyzz_store(a.wres + (size_t)win * 32, xyzz_add(v2, r2));
         }
     }
 }
@@ -536,17 +530,18 @@ struct FinalArgs {
     u32 *results;     // 16 u32 per MSM
 };
 
-// One warp per MSM: sum of its weighted windows, the carry, affine form.
+// One thread per MSM: Horner over its windows, sum_w 2^(c w) T_w with
+// c * (windows - 1) doublings, then the carry and the affine form.
 __global__ void k_final(FinalArgs f) {
-    const u32 lane = threadIdx.x & 31u;
-    const u32 m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u32 m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= f.M) return;
     const MsmDesc d = f.descs[m];
     Xyzz acc = xyzz_identity();
-    for (u32 w = lane; w < d.n_windows; w += 32) acc = xyzz_add(acc, xyzz_load(f.wres + (size_t)(d.win_base + w) * 32));
-#pragma unroll 1
-    for (u32 o = 16; o; o >>= 1) acc = xyzz_add(acc, xyzz_shfl_down(acc, o));
-    if (lane != 0) return;
+    for (int w = (int)d.n_windows - 1; w >= 0; w--) {
+        if (!xyzz_is_identity(acc))
+            for (u32 k = 0; k < d.c; k++) acc = xyzz_dbl(acc);
+        acc = xyzz_add(acc, xyzz_load(f.wres + (size_t)(d.win_base + w) * 32));
+    }
     if (f.carry) acc = xyzz_add(acc, xyzz_load(f.carry + (size_t)m * 32));
     if (f.emit_affine) {
         Affine r = xyzz_to_affine_fast(acc);

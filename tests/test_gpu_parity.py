@@ -304,11 +304,13 @@ def test_resident_window_tables(M):
     pts = O.gen_points(n, seed=21)
     ctx = _ctx(M, pts)
     ctx.precompute(10)
-    for m, c in ((n, 10), (n, 0), (777, 10), (n, 7), (1, 10)):
+    ctx.precompute(12)  # a second table set in the same allocation
+    ctx.precompute(10)  # already resident: no-op
+    for m, c in ((n, 10), (n, 12), (n, 0), (777, 10), (777, 12), (n, 7), (1, 10)):
         sc = O.gen_scalars(m, seed=21, stream=m + c)
         assert (host(ctx.msm_device(dev(sc), n=m, c=c)) == O.msm(pts[:m], sc)).all(), (m, c)
-    sizes = [5, 300, 9000, n]
-    b = ctx.batch(sizes, windows=[10, 0, 10, 0], graph=True)
+    sizes = [5, 300, 9000, n, 4000]
+    b = ctx.batch(sizes, windows=[10, 0, 10, 0, 12], graph=True)
     scal = [O.gen_scalars(s, seed=21, stream=500 + i) for i, s in enumerate(sizes)]
     out = host(b.run([dev(s) for s in scal])).reshape(-1, 16)
     for i, s in enumerate(sizes):
