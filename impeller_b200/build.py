@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-I" + os.path.join(ROOT, "include"),
            "-Wno-deprecated-gpu-targets"]
 
-SOURCES = ["engine.cu", "abi.cu", "aux_kernels.cu", "noalloc.cu"]
+SOURCES = ["engine.cu", "abi.cu", "aux_kernels.cu", "noalloc.cu", "serve.cu"]
 
 
 def nvcc() -> str:

@@ -184,7 +184,7 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
 }
 
 Plan::~Plan() {
-    if (staging) cudaFreeHost(staging);
+    if (staging && staging != ext_staging) cudaFreeHost(staging);
     if (staged) cudaEventDestroy(staged);
     for (auto &set : prof_sets)
         for (auto e : set) cudaEventDestroy(e);
@@ -228,7 +228,10 @@ cudaError_t Plan::read_profile(double *ms, u32 *runs) {
 }
 
 cudaError_t Plan::stage(const u32 *const *scalars) {
-    if (!staging) {
+    if (ext_staging && ext_cap >= tables.size()) {
+        staging = ext_staging;
+        if (!staged) CK(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+    } else if (!staging) {
         CK(cudaSetDevice(device));
         CK(cudaHostAlloc(&staging, tables.size(), cudaHostAllocPortable));
         CK(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
@@ -434,29 +437,8 @@ using namespace impeller;
 
 // -------------------------------------------------------------- contexts
 
-struct impeller_ctx {
-    int device = 0;
-    const u32 *points = nullptr;
-    u64 len = 0;
-    bool owns = false;
-    std::mutex mu;
-    void *scratch = nullptr;
-    size_t scratch_bytes = 0;
-    u32 *d_scalars = nullptr;  // staging for impeller_msm_host
-    u64 d_scalars_cap = 0;
-    u32 *d_result = nullptr;
-    cudaEvent_t done = nullptr;  // last run that used the scratch
-    bool profiling = false;
-    // Resident window tables: one allocation holding the points (region 0)
-    // followed by table sets; set for window c has W(c) tables of len points,
-    // table j = 2^(j*c) * P, starting at point index base.
-    u32 *tables = nullptr;
-    u64 tables_points = 0;  // points held by `tables`
-    std::vector<std::pair<u32, u32>> sets;  // (c, base)
-    std::map<std::pair<u32, u32>, std::unique_ptr<Plan>> plans;
-};
 
-static u32 ctx_set_base(const impeller_ctx *ctx, u32 c) {
+u32 impeller::ctx_set_base(const impeller_ctx *ctx, u32 c) {
     for (auto &s : ctx->sets)
         if (s.first == c) return s.second;
     return NONE;
@@ -464,7 +446,7 @@ static u32 ctx_set_base(const impeller_ctx *ctx, u32 c) {
 
 // With resident tables the context uses them for the sizes whose best
 // (measured) tables window is one of the sets it holds; other sizes run plain.
-static u32 ctx_window(const impeller_ctx *ctx, u64 n) {
+u32 impeller::ctx_window(const impeller_ctx *ctx, u64 n) {
     const u32 ct = table_window(n);
     if (ct && ctx_set_base(ctx, ct) != NONE) return ct;
     return default_window(n);
@@ -484,13 +466,13 @@ static cudaError_t ctx_reserve(impeller_ctx *ctx, size_t bytes, cudaStream_t st)
 
 // Shape of an MSM of n points with window c on this context: with a resident
 // table set for c every digit window shares one bucket set.
-static MsmShape ctx_shape(const impeller_ctx *ctx, u32 n, u32 c) {
+MsmShape impeller::ctx_shape(const impeller_ctx *ctx, u32 n, u32 c) {
     const u32 base = ctx_set_base(ctx, c);
     if (base != NONE) return MsmShape{n, c, 1, (u32)ctx->len, base};
     return MsmShape{n, c, 0, 0, 0};
 }
 
-static const u32 *ctx_point_base(const impeller_ctx *ctx) { return ctx->tables ? ctx->tables : ctx->points; }
+const u32 *impeller::ctx_point_base(const impeller_ctx *ctx) { return ctx->tables ? ctx->tables : ctx->points; }
 
 static Plan *ctx_plan(impeller_ctx *ctx, u32 n, u32 c) {
     auto key = std::make_pair(n, c);

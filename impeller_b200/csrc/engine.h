@@ -5,7 +5,11 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace impeller {
@@ -57,6 +61,14 @@ class Plan {
     // (stream: copy the image, run the kernels).  launch alone is what a
     // CUDA graph captures; stage before every replay.
     cudaError_t stage(const u32 *const *scalars);
+    // Use a caller-owned pinned buffer for the table image instead of one
+    // the plan allocates (and frees, which can synchronize the device).  The
+    // caller must not reuse it while a launch of this plan may still read it.
+    void set_staging(void *pinned, size_t cap) {
+        ext_staging = pinned;
+        ext_cap = cap;
+    }
+    size_t staging_bytes() const { return tables.size(); }
     // record_staged = false while capturing a CUDA graph: an event recorded
     // inside a capture cannot be waited on from the host, so the graph's
     // caller marks the staging buffer free after the graph launch instead.
@@ -92,6 +104,8 @@ class Plan {
 
   private:
     void *staging = nullptr;     // pinned copy of the tables
+    void *ext_staging = nullptr; // caller-owned staging (set_staging)
+    size_t ext_cap = 0;
     cudaEvent_t staged = nullptr;
     std::vector<unsigned char> tables;  // host image of the tables
     size_t desc_off = 0, win_off = 0, blk_off = 0;
@@ -108,4 +122,34 @@ cudaError_t combine_xyzz(const u32 *d_xyzz, u32 k, u32 *d_out, cudaStream_t stre
 // Window tables 2^(j*shift)*P for j in 1..n_tables-1, in place after table 0.
 cudaError_t precompute_tables(u32 *d_points, u64 n, u32 shift, u32 n_tables, cudaStream_t stream);
 
+}  // namespace impeller
+
+// Resident-SRS context (the C ABI's opaque impeller_ctx).
+struct impeller_ctx {
+    int device = 0;
+    const impeller::u32 *points = nullptr;
+    impeller::u64 len = 0;
+    bool owns = false;
+    std::mutex mu;
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    impeller::u32 *d_scalars = nullptr;  // staging for impeller_msm_host
+    impeller::u64 d_scalars_cap = 0;
+    impeller::u32 *d_result = nullptr;
+    cudaEvent_t done = nullptr;  // last run that used the scratch
+    bool profiling = false;
+    // Resident window tables: one allocation holding the points (region 0)
+    // followed by table sets; the set for window c has W(c) tables of len
+    // points, table j = 2^(j*c) * P, starting at point index base.
+    impeller::u32 *tables = nullptr;
+    impeller::u64 tables_points = 0;  // points held by `tables`
+    std::vector<std::pair<impeller::u32, impeller::u32>> sets;  // (c, base)
+    std::map<std::pair<impeller::u32, impeller::u32>, std::unique_ptr<impeller::Plan>> plans;
+};
+
+namespace impeller {
+u32 ctx_set_base(const impeller_ctx *ctx, u32 c);            // NONE if no set for c
+u32 ctx_window(const impeller_ctx *ctx, u64 n);              // window an MSM of n points uses
+MsmShape ctx_shape(const impeller_ctx *ctx, u32 n, u32 c);   // plan shape on this context
+const u32 *ctx_point_base(const impeller_ctx *ctx);          // points (and table sets) base
 }  // namespace impeller

@@ -51,6 +51,17 @@ SIGNATURES: dict[str, tuple] = {
     "impeller_batch_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "impeller_batch_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_uint32,
                                                    ctypes.POINTER(ctypes.c_uint32)]),
+    "impeller_server_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_uint32,
+                                              ctypes.c_uint32, ctypes.c_uint64]),
+    "impeller_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                              ctypes.POINTER(ctypes.c_uint64)]),
+    "impeller_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                            ctypes.POINTER(ctypes.c_double)]),
+    "impeller_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                            ctypes.POINTER(ctypes.c_double)]),
+    "impeller_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "impeller_server_inject_failures": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    "impeller_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "impeller_gen_scalars": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                             ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
     "impeller_gen_points": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,

@@ -411,3 +411,82 @@ def n_precompute(window_size: int, target_window: int) -> int:
 
 def window_count(c: int) -> int:
     return math.ceil(BN254_BITS / c)
+
+
+# ------------------------------------------------------ continuous batching
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("points", ctypes.c_uint64),
+                ("peak_bytes", ctypes.c_uint64), ("budget_bytes", ctypes.c_uint64), ("mean_batch", ctypes.c_double),
+                ("span_s", ctypes.c_double), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("max_concurrent", ctypes.c_uint64)]
+
+
+class MsmServer:
+    """Continuous-batching MSM server on a context (impeller_server_* C ABI).
+
+    submit() queues a job and returns at once; jobs that arrive while others
+    run are admitted as batch slots and HBM free up and run overlapped with
+    them; wait() returns the 16-word result and the job's latency."""
+
+    def __init__(self, ctx: MsmContext, max_batch: int = 64, max_inflight: int = 3, hbm_budget: int = 0):
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(L.impeller_server_create(ctypes.byref(h), ctx.handle, max_batch, max_inflight, hbm_budget),
+                   "impeller_server_create")
+        self.handle = h
+        self.ctx = ctx
+        self._keep: dict = {}
+
+    def submit(self, h_scalars: np.ndarray) -> int:
+        sc = np.ascontiguousarray(h_scalars, dtype=np.uint32).reshape(-1, 8)
+        jid = ctypes.c_uint64()
+        _lib.check(_lib.load().impeller_server_submit(self.handle, sc.ctypes.data, sc.shape[0], ctypes.byref(jid)),
+                   "impeller_server_submit")
+        self._keep[jid.value] = sc
+        return jid.value
+
+    def submit_raw(self, ptr: int, n: int) -> int:
+        """Submit scalars the caller keeps alive (host pointer, n x 8 u32)."""
+        jid = ctypes.c_uint64()
+        _lib.check(_lib.load().impeller_server_submit(self.handle, ptr, n, ctypes.byref(jid)),
+                   "impeller_server_submit")
+        return jid.value
+
+    def wait(self, job: int):
+        out = np.zeros(16, dtype=np.uint32)
+        lat = ctypes.c_double()
+        rc = _lib.load().impeller_server_wait(self.handle, job, out.ctypes.data, ctypes.byref(lat))
+        self._keep.pop(job, None)
+        _lib.check(rc, "MSM job")
+        return out, lat.value
+
+    def poll(self, job: int):
+        out = np.zeros(16, dtype=np.uint32)
+        lat = ctypes.c_double()
+        rc = _lib.load().impeller_server_poll(self.handle, job, out.ctypes.data, ctypes.byref(lat))
+        if rc == 600:  # cudaErrorNotReady
+            return None
+        self._keep.pop(job, None)
+        _lib.check(rc, "MSM job")
+        return out, lat.value
+
+    def inject_failures(self, batches: int) -> None:
+        _lib.check(_lib.load().impeller_server_inject_failures(self.handle, batches), "inject")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _lib.check(_lib.load().impeller_server_get_stats(self.handle, ctypes.byref(st)), "stats")
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if self.handle:
+            _lib.load().impeller_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -148,6 +148,44 @@ cudaError_t impeller_batch_profile(impeller_batch *b, int enable);
 cudaError_t impeller_batch_profile_read(impeller_batch *b, double *ms_per_phase, uint32_t nphase, uint32_t *runs);
 
 /* ------------------------------------------------------------------------
+ * Continuous-batching server over a context (additive; the reference serves
+ * whole proofs through its scheduler, scheduler/src/scheduler/core.rs:419-580,
+ * and has no MSM-level serving).  Jobs are admitted in arrival order while
+ * one of max_inflight batch slots is free and their device footprint fits the
+ * HBM budget (0: free memory at creation minus 1 GiB); each admitted group
+ * (at most max_batch jobs) runs as one batch on its own stream, so batches on
+ * the GPU at the same time overlap.  Each job uses the window (and resident
+ * table set) the context would use alone, so its result is the same alone and
+ * in any mix.  The caller keeps h_scalars alive and unchanged until the job's
+ * result has been taken.
+ */
+typedef struct impeller_server impeller_server;
+typedef struct impeller_server_stats {
+    uint64_t submitted, completed, rejected, failed, batches, points, peak_bytes, budget_bytes;
+    double mean_batch; /* jobs per batch */
+    double span_s;     /* first submission to last completion */
+    double p50_ms, p99_ms, mean_ms, max_ms; /* submission-to-result latency */
+    uint64_t max_concurrent;                /* most batches on the GPU at once */
+} impeller_server_stats;
+
+cudaError_t impeller_server_create(impeller_server **out, impeller_ctx *ctx, uint32_t max_batch,
+                                   uint32_t max_inflight, uint64_t hbm_budget);
+/* Queue one MSM over the first n resident points.  Refuses (and counts) n == 0,
+ * n > SRS length, NULL scalars (cudaErrorInvalidValue) and jobs whose device
+ * footprint exceeds the budget (cudaErrorMemoryAllocation). */
+cudaError_t impeller_server_submit(impeller_server *s, const uint32_t *h_scalars, uint64_t n, uint64_t *job_id);
+/* Block until the job is done; copy its 16-word result; return its status. */
+cudaError_t impeller_server_wait(impeller_server *s, uint64_t job_id, uint32_t *h_result, double *latency_ms);
+/* Like wait, but cudaErrorNotReady while the job is pending. */
+cudaError_t impeller_server_poll(impeller_server *s, uint64_t job_id, uint32_t *h_result, double *latency_ms);
+cudaError_t impeller_server_get_stats(impeller_server *s, impeller_server_stats *out);
+/* Fail the next `batches` batches on the host, without GPU work (failure
+ * handling tests: their jobs complete with cudaErrorLaunchFailure). */
+cudaError_t impeller_server_inject_failures(impeller_server *s, uint32_t batches);
+/* Drain queued and running jobs, then stop. */
+cudaError_t impeller_server_destroy(impeller_server *s);
+
+/* ------------------------------------------------------------------------
  * Seeded synthetic inputs, computed on the device (definitions shared with
  * the CPU oracle: splitmix64 counter streams, uniform Fr, the skewed
  * witness-like mix, P_i = r_i * G). */
