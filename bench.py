@@ -223,7 +223,8 @@ def main():
     dev = local
     stream = torch.cuda.current_stream()
 
-    pts = M.gen_points_device(n, seed=0, device=dev)
+    srs_log2 = max(args.log2n, 23 if not args.no_extras else args.log2n)
+    pts = M.gen_points_device(1 << srs_log2, seed=0, device=dev)  # SRS; the MSM uses its first n points
     V = 4  # rotating scalar vectors: 4 x 128 MiB + 256 MiB of points, inputs > L2
     scal = [M.gen_scalars_device(n, seed=0, stream_id=1 + v, device=dev) for v in range(V)]
     ctx = M.MsmContext(pts, device=dev)
@@ -317,10 +318,11 @@ def main():
         }
 
     if not args.no_extras and rank == 0:
-        line["e2e"] = e2e_reference_abi(M, pts, scal[0], n, c, args)
+        line["e2e"] = e2e_reference_abi(M, pts[:n], scal[0], n, c, args)
         line["e2e_resident_srs"] = e2e_resident(M, ctx, scal[0], n, c, args)
         line["batched"] = batched_vs_per_call(M, ctx, dev, args)
-        pts_host = M.to_host(pts[: 1 << 20]).reshape(-1, 16)
+        line["served"] = served_stream(M, ctx, dev, args)
+        pts_host = M.to_host(pts[: 1 << 20]).reshape(-1, 16)  # noqa: E501
         sc_host = M.to_host(scal[0][: 1 << 20]).reshape(-1, 8)
         line["cpu_baseline"] = cpu_baseline(pts_host, sc_host)
     ctx.close()
@@ -372,6 +374,49 @@ def e2e_resident(M, ctx, d_scal, n, c, args) -> dict:
     dt = (time.perf_counter() - t0) / steps
     return {"value": n / dt, "unit": UNIT, "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": 64,
             "ms_per_step": dt * 1e3, "api": "impeller_msm_host (points resident), pinned scalars, wall clock"}
+
+
+def served_stream(M, ctx, dev, args, seconds: float = 6.0, rate: float = 200.0) -> dict:
+    """Poisson arrivals (mean 200 jobs/s) of MSM jobs with sizes log-uniform in
+    [2^12, 2^23] over the resident 2^23-point SRS, served with continuous
+    batching; every job's scalars are a slice of one pinned host buffer."""
+    import torch
+    nmax = 1 << 23
+    for ct in sorted({M.table_window(1 << k) for k in range(12, 24)} - {0}):
+        ctx.precompute(ct)
+    host = torch.empty((nmax, 8), dtype=torch.int32, pin_memory=True)
+    host.copy_(M.gen_scalars_device(nmax, seed=0, stream_id=77, device=dev).cpu())
+    base = host.data_ptr()
+    rng = np.random.default_rng(0)
+    jobs = []
+    t = 0.0
+    while t < seconds:
+        t += rng.exponential(1.0 / rate)
+        n = int(round(2 ** rng.uniform(12, 23)))
+        off = int(rng.integers(0, nmax - n + 1))
+        jobs.append((t, n, off))
+    srv = M.MsmServer(ctx, max_batch=64, max_inflight=3)
+    ids = []
+    t0 = time.perf_counter()
+    for (ta, n, off) in jobs:
+        delay = ta - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit_raw(base + off * 32, n))
+    results = [srv.wait(j)[0] for j in ids]
+    st = srv.stats()
+    srv.close()
+    # bit-exactness in the mix: a sample of jobs again, alone
+    checks = rng.choice(len(jobs), size=min(12, len(jobs)), replace=False)
+    same = all(np.array_equal(results[i], ctx.msm_host(host[jobs[i][2]: jobs[i][2] + jobs[i][1]].numpy()
+                                                          .view(np.uint32))) for i in checks)
+    total = sum(n for _, n, _ in jobs)
+    return {"workload": f"Poisson {rate:g} jobs/s for {seconds:g} s, n log-uniform in [2^12, 2^23], 2^23 SRS",
+            "jobs": len(jobs), "points": total, "points_per_s": total / st["span_s"] if st["span_s"] else None,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"], "mean_ms": st["mean_ms"],
+            "batches": st["batches"], "mean_batch": st["mean_batch"], "max_concurrent": st["max_concurrent"],
+            "peak_hbm_bytes": st["peak_bytes"], "sample_same_alone_and_in_mix": bool(same),
+            "sample_checked": int(len(checks))}
 
 
 def batched_vs_per_call(M, ctx, dev, args) -> dict:
