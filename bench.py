@@ -130,6 +130,12 @@ def signed_digit_stats(scalars_canonical: np.ndarray, c: int, shared: bool = Fal
     return nonzero, (len(used) if shared else buckets)
 
 
+# DRAM bytes per k_accumulate launch, measured with ncu (dram__bytes_read.sum
+# + dram__bytes_write.sum) on the same kernel at n = 2^21 with window tables
+# c = 20 (3.604 GB + 0.079 GB) and scaled to n = 2^22 by the number of mixed
+# additions (traffic grows in proportion): used when the run matches.
+NCU_TRAFFIC_2E22_TABLES_C20 = 7.37e9
+
 # One Fq Montgomery product is 8 rows x (8 products a_j*b_i, 1 for the
 # reduction factor, 8 products m*N_j) = 136 32x32->64-bit partial products;
 # a mixed XYZZ + affine addition (madd-2008-s) is 10 Montgomery products.
@@ -306,7 +312,10 @@ def main():
             "gpu_launches": args.steps * 10,
             "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
             "roofline": {"bound": "imad", "kernel": "k_accumulate", "achieved": achieved, "peak": peak.value,
-                         "unit": "G 32x32->64 products/s", "frac": achieved / peak.value, "traffic": None,
+                         "unit": "G 32x32->64 products/s", "frac": achieved / peak.value,
+                         "traffic": NCU_TRAFFIC_2E22_TABLES_C20 if (args.log2n == 22 and c_tab == 20 and c == 20)
+                         else None,
+                         "algorithmic_bytes": madds * (64 + 4),
                          "per_launch": {"madds": madds, "products_per_madd": MULS_PER_MADD * PRODUCTS_PER_MUL,
                                         "ms": acc_ms},
                          "peak_source": "impeller_imad_peak: independent mul.wide.u32 products, measured live"},
