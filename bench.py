@@ -179,6 +179,21 @@ def run_reference(args, rank, world):
 
 # ------------------------------------------------------------------ main
 
+def max_over_ranks(ms: float, dist=None, device=None) -> float:
+    """The slowest rank's time (every rank runs the same collective)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(n_per_rank: int, world: int, ms_max: float) -> float:
+    """Weak scaling: every rank runs its own n-point MSM; whole-job points/s."""
+    return world * n_per_rank / (ms_max / 1e3)
+
+
 def cpu_baseline(pts_host: np.ndarray, scal_host: np.ndarray) -> dict:
     from oracle import oracle as O
     cores = os.cpu_count() or 1
@@ -266,11 +281,8 @@ def main():
     clocks = sampler.stop()
     barrier()
     ms = e0.elapsed_time(e1) / args.steps
-    ms_t = torch.tensor([ms], device=f"cuda:{dev}")
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * n / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dist, device=f"cuda:{dev}")
+    value = replica_value(n, world, ms_max)
 
     phases = (ctypes.c_double * 8)()
     runs = ctypes.c_uint32()
