@@ -136,11 +136,12 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     p.nwins = (u32)wins.size();
     p.nrblocks = (u32)rblocks.size();
 
-    // accumulate: persistent threads, at least 8 entries each
-    const u32 full_blocks = (u32)sms * 2;
+    // accumulate: persistent threads (every resident slot), at least 8 entries each
+    const u32 full_blocks = (u32)sms * ACCUM_PER_SM;
     const u64 want_threads = (entries + 7) / 8;
-    p.accum_blocks = (u32)std::max<u64>(1, std::min<u64>(full_blocks, (want_threads + 255) / 256));
-    p.accum_block = 256;
+    p.accum_blocks =
+        (u32)std::max<u64>(1, std::min<u64>(full_blocks, (want_threads + ACCUM_BLOCK - 1) / ACCUM_BLOCK));
+    p.accum_block = ACCUM_BLOCK;
     const u32 T = p.accum_blocks * p.accum_block;
     p.long_cap = T;
     p.hist_grid_x = (u32)std::max<u64>(1, std::min<u64>((u64)sms * 8, (nmax + 255) / 256));

@@ -266,7 +266,20 @@ __device__ __forceinline__ Affine load_entry_point(const u32 *__restrict__ point
 // Otherwise the slice leaves a record: slot 2t for a piece that continues a
 // bucket begun in an earlier slice, slot 2t+1 for a piece whose bucket begins
 // in this slice and continues in later ones.
-__global__ void __launch_bounds__(256, 2) k_accumulate(AccumArgs a) {
+// One block of 384 threads per SM: 146 registers per thread with no spills,
+// 12 warps spread evenly over the SM's four schedulers.  Measured on B200 at
+// 2^22 this beats 2 x 256 threads at 128 registers (which spill) by 4%, and
+// 320-, 352- and 256-thread single blocks by 8-20%.
+#ifndef ACCUM_THREADS
+#define ACCUM_THREADS 384
+#endif
+#ifndef ACCUM_BLOCKS_PER_SM
+#define ACCUM_BLOCKS_PER_SM 1
+#endif
+static constexpr u32 ACCUM_BLOCK = ACCUM_THREADS;
+static constexpr u32 ACCUM_PER_SM = ACCUM_BLOCKS_PER_SM;
+
+__global__ void __launch_bounds__(ACCUM_THREADS, ACCUM_BLOCKS_PER_SM) k_accumulate(AccumArgs a) {
     const u32 T = gridDim.x * blockDim.x;
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 E = a.offsets[a.nb];
