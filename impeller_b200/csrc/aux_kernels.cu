@@ -79,7 +79,7 @@ __device__ Fr uniform_fr(u64 key, u64 idx) {
         l.l[i] = lo[i];
     }
     Fr t = fe_mul<FrP>(h, fr_r2());  // hi * 2^256 mod r
-    return fe_add<FrP>(l, t);
+    return fe_canon<FrP>(fe_add<FrP>(l, t));
 }
 
 __global__ void k_gen_scalars(u32 *out, u64 n, u64 seed, u64 stream, int dist, u64 start, int mont) {
@@ -99,7 +99,7 @@ __global__ void k_gen_scalars(u32 *out, u64 n, u64 seed, u64 stream, int dist, u
             }
         }
         if (uniform) v = uniform_fr(key, idx);
-        if (mont) v = fe_mul<FrP>(v, fr_r2());
+        if (mont) v = fe_canon<FrP>(fe_mul<FrP>(v, fr_r2()));
         fe_store(out + 8 * i, v);
     }
 }
@@ -141,10 +141,10 @@ __global__ void k_test_field(int field, int op, const u32 *a, const u32 *b, u32 
     if (i >= count) return;
     if (field == 0) {
         Fq x = fe_load<FqP>(a + 8 * i), y = b ? fe_load<FqP>(b + 8 * i) : fe_zero<FqP>();
-        fe_store(out + 8 * i, test_op<FqP>(op, x, y, fq_r2()));
+        fe_store(out + 8 * i, fe_canon<FqP>(test_op<FqP>(op, x, y, fq_r2())));
     } else {
         Fr x = fe_load<FrP>(a + 8 * i), y = b ? fe_load<FrP>(b + 8 * i) : fe_zero<FrP>();
-        fe_store(out + 8 * i, test_op<FrP>(op, x, y, fr_r2()));
+        fe_store(out + 8 * i, fe_canon<FrP>(test_op<FrP>(op, x, y, fr_r2())));
     }
 }
 

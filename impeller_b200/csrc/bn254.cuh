@@ -12,6 +12,14 @@
 // running value stays below 3N < 2^256 even for inputs in [0, 2N), so nine
 // words hold every intermediate and no carry ever leaves word 8.
 //
+// Reduction is lazy: between operations a field value is any representative
+// in [0, 2N).  For inputs below 2N the Montgomery product is below
+// (4N^2 + R N) / R < 2N (as 4N < R), so it skips the final conditional
+// subtraction; addition and subtraction work modulo 2N.  A value is zero mod N
+// when it is 0 or N (fe_is_zero).  fe_canon gives the representative in
+// [0, N); every value that leaves the arithmetic (affine results, generated
+// scalars, test outputs) is canonical.
+//
 // Curve points use XYZZ coordinates (x = X/ZZ, y = Y/ZZZ, ZZ^3 = ZZZ^2), the
 // point representation of core/src/common/curve/src/curve_xyzz.cuh:252-418,
 // with the Explicit-Formulas Database's madd-2008-s, add-2008-s,
@@ -34,6 +42,9 @@ struct FqP {
     // R mod p (Montgomery one)
     static constexpr u32 R0 = 0xc58f0d9du, R1 = 0xd35d438du, R2 = 0xf5c70b3du, R3 = 0x0a78eb28u;
     static constexpr u32 R4 = 0x7879462cu, R5 = 0x666ea36fu, R6 = 0x9a07df2fu, R7 = 0x0e0a77c1u;
+    // 2p
+    static constexpr u32 D0 = 0xb0f9fa8eu, D1 = 0x7841182du, D2 = 0xd0e3951au, D3 = 0x2f02d522u;
+    static constexpr u32 D4 = 0x0302b0bbu, D5 = 0x70a08b6du, D6 = 0xc2634053u, D7 = 0x60c89ce5u;
 };
 
 struct FrP {
@@ -42,6 +53,9 @@ struct FrP {
     static constexpr u32 INV = 0xefffffffu;  // -r^{-1} mod 2^32
     static constexpr u32 R0 = 0x4ffffffbu, R1 = 0xac96341cu, R2 = 0x9f60cd29u, R3 = 0x36fc7695u;
     static constexpr u32 R4 = 0x7879462eu, R5 = 0x666ea36fu, R6 = 0x9a07df2fu, R7 = 0x0e0a77c1u;
+    // 2r
+    static constexpr u32 D0 = 0xe0000002u, D1 = 0x87c3eb27u, D2 = 0xf372e122u, D3 = 0x5067d090u;
+    static constexpr u32 D4 = 0x0302b0bau, D5 = 0x70a08b6du, D6 = 0xc2634053u, D7 = 0x60c89ce5u;
 };
 
 template <class F>
@@ -68,18 +82,20 @@ __host__ __device__ __forceinline__ Fe<F> fe_one() {
     return r;
 }
 
+// Zero test for a canonical value (in [0, N)).
 template <class F>
-__device__ __forceinline__ bool fe_is_zero(const Fe<F> &a) {
+__device__ __forceinline__ bool fe_is_zero_canonical(const Fe<F> &a) {
     u32 x = (a.l[0] | a.l[1]) | (a.l[2] | a.l[3]) | (a.l[4] | a.l[5]) | (a.l[6] | a.l[7]);
     return x == 0;
 }
 
+// Zero test for a value in [0, 2N): 0 or N.
 template <class F>
-__device__ __forceinline__ bool fe_eq(const Fe<F> &a, const Fe<F> &b) {
-    u32 x = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) x |= a.l[i] ^ b.l[i];
-    return x == 0;
+__device__ __forceinline__ bool fe_is_zero(const Fe<F> &a) {
+    u32 x = (a.l[0] | a.l[1]) | (a.l[2] | a.l[3]) | (a.l[4] | a.l[5]) | (a.l[6] | a.l[7]);
+    u32 y = ((a.l[0] ^ F::M0) | (a.l[1] ^ F::M1)) | ((a.l[2] ^ F::M2) | (a.l[3] ^ F::M3)) |
+            ((a.l[4] ^ F::M4) | (a.l[5] ^ F::M5)) | ((a.l[6] ^ F::M6) | (a.l[7] ^ F::M7));
+    return x == 0 || y == 0;
 }
 
 // r = (t < N) ? t : t - N, for t < 2N.
@@ -102,6 +118,35 @@ __device__ __forceinline__ void fe_reduce_once(Fe<F> &r, const u32 t[8]) {
     // bw == 0xffffffff when t < N: keep t
 #pragma unroll
     for (int i = 0; i < 8; i++) r.l[i] = bw ? t[i] : d[i];
+}
+
+// r = (t < 2N) ? t : t - 2N, for t < 4N.
+template <class F>
+__device__ __forceinline__ void fe_reduce_2n(Fe<F> &r, const u32 t[8]) {
+    u32 d[8], bw;
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+          "=r"(bw)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]),
+          "n"(F::D0), "n"(F::D1), "n"(F::D2), "n"(F::D3), "n"(F::D4), "n"(F::D5), "n"(F::D6), "n"(F::D7));
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.l[i] = bw ? t[i] : d[i];
+}
+
+// The canonical representative in [0, N) of a value in [0, 2N).
+template <class F>
+__device__ __forceinline__ Fe<F> fe_canon(const Fe<F> &a) {
+    Fe<F> r;
+    fe_reduce_once<F>(r, a.l);
+    return r;
 }
 
 // Even/odd row of wide products: t[0..8] += a * bi.  The eight 64-bit
@@ -129,9 +174,10 @@ __device__ __forceinline__ void fe_reduce_once(Fe<F> &r, const u32 t[8]) {
           "+r"(t[7]), "+r"(t[8])                                                                     \
         : x0, x1, x2, x3, x4, x5, x6, x7, "r"(y))
 
-// Montgomery product a*b*R^{-1} mod N, fully reduced (inputs reduced):
+// Montgomery product a*b*R^{-1} mod N in [0, 2N) for inputs in [0, 2N):
 // per row of b, the even/odd wide-product row for a*b[i], the reduction
-// factor m, the even/odd row for m*N, a one-word shift.
+// factor m, the even/odd row for m*N, a one-word shift.  No final
+// subtraction (lazy reduction).
 template <class F>
 __device__ __forceinline__ Fe<F> fe_mul_inline(const Fe<F> &a, const Fe<F> &b) {
     u32 t[9];
@@ -149,7 +195,8 @@ __device__ __forceinline__ Fe<F> fe_mul_inline(const Fe<F> &a, const Fe<F> &b) {
         t[8] = 0;
     }
     Fe<F> r;
-    fe_reduce_once<F>(r, t);
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.l[i] = t[i];
     return r;
 }
 
@@ -168,7 +215,9 @@ __device__ __forceinline__ Fe<F> fe_sqr(const Fe<F> &a) {
     return fe_mul<F>(a, a);
 }
 
-// Leave Montgomery form: a * R^{-1} mod N (Montgomery reduction only).
+// Leave Montgomery form: a * R^{-1} mod N, canonical, for a in [0, 2N)
+// (Montgomery reduction only; the sum stays at or below N before the final
+// subtraction).
 template <class F>
 __device__ __forceinline__ Fe<F> fe_from_mont(const Fe<F> &a) {
     u32 t[9];
@@ -224,7 +273,7 @@ __device__ __forceinline__ Fe<F> fe_add(const Fe<F> &a, const Fe<F> &b) {
           "r"(a.l[7]), "r"(b.l[0]), "r"(b.l[1]), "r"(b.l[2]), "r"(b.l[3]), "r"(b.l[4]), "r"(b.l[5]),
           "r"(b.l[6]), "r"(b.l[7]));
     Fe<F> r;
-    fe_reduce_once<F>(r, s);
+    fe_reduce_2n<F>(r, s);  // a + b < 4N < 2^256
     return r;
 }
 
@@ -246,7 +295,7 @@ __device__ __forceinline__ Fe<F> fe_sub(const Fe<F> &a, const Fe<F> &b) {
           "r"(a.l[7]), "r"(b.l[0]), "r"(b.l[1]), "r"(b.l[2]), "r"(b.l[3]), "r"(b.l[4]), "r"(b.l[5]),
           "r"(b.l[6]), "r"(b.l[7]));
     Fe<F> r;
-    // add N back when the subtraction borrowed (bw = 0xffffffff)
+    // add 2N back when the subtraction borrowed (bw = 0xffffffff)
     asm("add.cc.u32  %0, %8, %16;\n\t"
         "addc.cc.u32 %1, %9, %17;\n\t"
         "addc.cc.u32 %2, %10, %18;\n\t"
@@ -258,8 +307,8 @@ __device__ __forceinline__ Fe<F> fe_sub(const Fe<F> &a, const Fe<F> &b) {
         : "=r"(r.l[0]), "=r"(r.l[1]), "=r"(r.l[2]), "=r"(r.l[3]), "=r"(r.l[4]), "=r"(r.l[5]), "=r"(r.l[6]),
           "=r"(r.l[7])
         : "r"(d[0]), "r"(d[1]), "r"(d[2]), "r"(d[3]), "r"(d[4]), "r"(d[5]), "r"(d[6]), "r"(d[7]),
-          "r"(F::M0 & bw), "r"(F::M1 & bw), "r"(F::M2 & bw), "r"(F::M3 & bw), "r"(F::M4 & bw),
-          "r"(F::M5 & bw), "r"(F::M6 & bw), "r"(F::M7 & bw));
+          "r"(F::D0 & bw), "r"(F::D1 & bw), "r"(F::D2 & bw), "r"(F::D3 & bw), "r"(F::D4 & bw),
+          "r"(F::D5 & bw), "r"(F::D6 & bw), "r"(F::D7 & bw));
     return r;
 }
 
@@ -342,7 +391,7 @@ __device__ __forceinline__ void u256_sub(u32 a[8], const u32 b[8]) {
         : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
 }
 
-// x = x / 2 mod N for x < N (N odd): if x is odd, (x + N) / 2.
+// x = x / 2 mod N for x < 2N (N odd): if x is odd, (x + N) / 2 < 3N / 2.
 template <class F>
 __device__ __forceinline__ void fe_half(u32 x[8]) {
     if (x[0] & 1u) {
@@ -366,8 +415,9 @@ __device__ __forceinline__ void fe_half(u32 x[8]) {
 }
 
 template <class F>
-__device__ __noinline__ Fe<F> fe_inv_binary(const Fe<F> &a, const Fe<F> &r3) {
-    if (fe_is_zero(a)) return a;
+__device__ __noinline__ Fe<F> fe_inv_binary(const Fe<F> &a_in, const Fe<F> &r3) {
+    const Fe<F> a = fe_canon<F>(a_in);
+    if (fe_is_zero_canonical(a)) return a;
     u32 u[8], v[8];
     Fe<F> x1 = fe_zero<F>(), x2 = fe_zero<F>();
     x1.l[0] = 1;
@@ -432,7 +482,8 @@ struct Xyzz {
     Fq x, y, zz, zzz;
 };
 
-__device__ __forceinline__ bool affine_is_identity(const Affine &a) { return fe_is_zero(a.y); }
+// Affine points come from memory in canonical form; negation keeps 0 at 0.
+__device__ __forceinline__ bool affine_is_identity(const Affine &a) { return fe_is_zero_canonical(a.y); }
 
 __device__ __forceinline__ Xyzz xyzz_identity() {
     Xyzz r;
@@ -569,8 +620,8 @@ __device__ __forceinline__ Affine xyzz_to_affine_fast(const Xyzz &p) {
     }
     Fq a = fe_inv_binary<FqP>(p.zzz, fq_r3());
     Fq b = fe_sqr(fe_mul(p.zz, a));
-    r.x = fe_mul(p.x, b);
-    r.y = fe_mul(p.y, a);
+    r.x = fe_canon(fe_mul(p.x, b));
+    r.y = fe_canon(fe_mul(p.y, a));
     return r;
 }
 
@@ -584,8 +635,8 @@ __device__ __forceinline__ Affine xyzz_to_affine(const Xyzz &p) {
     }
     Fq a = fe_inv(p.zzz);
     Fq b = fe_sqr(fe_mul(p.zz, a));
-    r.x = fe_mul(p.x, b);
-    r.y = fe_mul(p.y, a);
+    r.x = fe_canon(fe_mul(p.x, b));
+    r.y = fe_canon(fe_mul(p.y, a));
     return r;
 }
 
