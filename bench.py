@@ -330,7 +330,7 @@ def main():
                          "algorithmic_bytes": madds * (64 + 4),
                          "per_launch": {"madds": madds, "products_per_madd": MULS_PER_MADD * PRODUCTS_PER_MUL,
                                         "ms": acc_ms},
-                         "peak_source": "impeller_imad_peak: independent mul.wide.u32 products, measured live"},
+                         "peak_source": "impeller_imad_peak: independent Fq Montgomery products (4 chains/thread, 136 partial products each), measured live"},
             "roofline_sort": {"bound": "hbm", "kernels": "k_histogram+k_scan+k_scatter",
                               "achieved": sort_bytes / (sort_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                               "frac": sort_bytes / (sort_ms * 1e-3) / 1e9 / hbm_peak,

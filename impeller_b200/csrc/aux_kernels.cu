@@ -170,32 +170,32 @@ __global__ void k_test_point(int op, const u32 *p, const u32 *q, u32 *out, u64 c
     affine_store(out + 16 * i, xyzz_to_affine(r));
 }
 
-// Peak of the 32x32 -> 64-bit multiply (mul.wide.u32) the Montgomery product
-// is built from: 16 independent products per thread per step, folded into
-// accumulators with xor so that no carry arithmetic competes for issue.
+// Throughput ceiling of the Montgomery product itself: four independent
+// chains of Fq products per thread at full occupancy, nothing else in the
+// loop.  A product is 136 32x32 -> 64-bit partial products (64 for a*b, 64
+// for m*N, 8 reduction factors).
 __global__ void k_imad_peak(u32 *out, u32 iters, u32 seed) {
-    u32 a[8];
-    u64 acc[8];
+    Fq acc[4], m;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        a[k] = seed * (threadIdx.x + 3 * k + 1) + blockIdx.x;
-        acc[k] = a[k];
+    for (int k = 0; k < 8; k++) m.l[k] = seed * (threadIdx.x + 5 * k + 1) + blockIdx.x;
+    m.l[7] &= 0x3fffffffu;  // below 2p
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[r].l[k] = m.l[(k + r) & 7] ^ (u32)r;
+        acc[r].l[7] &= 0x3fffffffu;
     }
 #pragma unroll 1
     for (u32 it = 0; it < iters; it++) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            u64 p, q;
-            asm volatile("mul.wide.u32 %0, %1, %2;" : "=l"(p) : "r"(a[k]), "r"(a[(k + 1) & 7]));
-            asm volatile("mul.wide.u32 %0, %1, %2;" : "=l"(q) : "r"(a[k]), "r"(a[(k + 3) & 7]));
-            acc[k] ^= p ^ q;
-            a[k] += (u32)it;
-        }
+        for (int r = 0; r < 4; r++) acc[r] = fe_mul<FqP>(acc[r], m);
     }
-    u64 x = 0;
+    u32 v = 0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) x ^= acc[k];
-    if (x == 0x12345678ull) out[blockIdx.x * blockDim.x + threadIdx.x] = (u32)x;
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) v ^= acc[r].l[k];
+    if (v == 0x12345678u) out[blockIdx.x * blockDim.x + threadIdx.x] = v;
 }
 
 // Dependent chains of one operation on one thread (op 0 Fq product,
@@ -262,7 +262,7 @@ cudaError_t impeller_imad_peak(int device, double *gops) {
     if (e != cudaSuccess) return e;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const u32 blocks = (u32)sms * 8, threads = 256, iters = 1u << 14;
+    const u32 blocks = (u32)sms * 8, threads = 256, iters = 1u << 11;
     u32 *out = nullptr;
     if ((e = cudaMalloc(&out, (size_t)blocks * threads * 4)) != cudaSuccess) return e;
     cudaEvent_t t0, t1;
@@ -284,7 +284,7 @@ cudaError_t impeller_imad_peak(int device, double *gops) {
     cudaEventDestroy(t1);
     cudaFree(out);
     if (e != cudaSuccess) return e;
-    *gops = (double)blocks * threads * iters * 16.0 / (best * 1e-3) / 1e9;
+    *gops = (double)blocks * threads * iters * 4.0 * 136.0 / (best * 1e-3) / 1e9;
     return cudaSuccess;
 }
 

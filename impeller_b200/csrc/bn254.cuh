@@ -3,12 +3,12 @@
 // Field elements are 8 little-endian 32-bit limbs in Montgomery form with
 // R = 2^256, the layout of the reference's mont::Element
 // (core/src/common/mont/src/field.cuh:906-1204) and of its C ABI.
-// Multiplication is coarsely integrated operand scanning: per row of b, eight
-// 32x32->64 wide products of a*b[i] (one integer-multiply-pipe instruction
-// each) added in two carry chains on the ALU, the reduction factor m, and the
-// same for m*N.  Measured on B200 this mix (144 multiply-pipe + 272 ALU
-// instructions per product) beats separate mad.lo / mad.hi carry chains
-// (285 + 267), whose multiply pipe saturates first.  Because N < 2^254 the
+// Multiplication is coarsely integrated operand scanning: per row of b, the
+// products a_j*b[i] are added into the running value by lo/hi multiply-add
+// pairs with carry (even j in one chain, odd j in a second), then the
+// reduction factor m and the same for m*N.  Measured on B200, the
+// accumulation loop runs 10% faster this way than with 64-bit mul.wide
+// products added by separate ALU carry chains.  Because N < 2^254 the
 // running value stays below 3N < 2^256 even for inputs in [0, 2N), so nine
 // words hold every intermediate and no carry ever leaves word 8.
 //
@@ -149,64 +149,120 @@ __device__ __forceinline__ Fe<F> fe_canon(const Fe<F> &a) {
     return r;
 }
 
-// Even/odd row of wide products: t[0..8] += a * bi.  The eight 64-bit
-// products a_j * bi are formed with mul.wide; the even-j products tile words
-// 0..7 exactly (lo of a_j at word j, hi at j+1), the odd-j products tile words
-// 1..8, so one carry chain adds each tiling.  One multiply per 32x32 product
-// instead of a separate lo and hi multiply-add; the carries run on the
-// integer ALU.
-#define BN_EO_ROW(t, x0, x1, x2, x3, x4, x5, x6, x7, y)                                             \
-    asm("{\n\t.reg .u64 p0,p1,p2,p3,p4,p5,p6,p7;\n\t"                                                 \
-        ".reg .u32 l0,h0,l1,h1,l2,h2,l3,h3,l4,h4,l5,h5,l6,h6,l7,h7;\n\t"                               \
-        "mul.wide.u32 p0, %9, %17;\n\tmul.wide.u32 p1, %10, %17;\n\tmul.wide.u32 p2, %11, %17;\n\t"  \
-        "mul.wide.u32 p3, %12, %17;\n\tmul.wide.u32 p4, %13, %17;\n\tmul.wide.u32 p5, %14, %17;\n\t" \
-        "mul.wide.u32 p6, %15, %17;\n\tmul.wide.u32 p7, %16, %17;\n\t"                                \
-        "mov.b64 {l0,h0}, p0;\n\tmov.b64 {l1,h1}, p1;\n\tmov.b64 {l2,h2}, p2;\n\t"                   \
-        "mov.b64 {l3,h3}, p3;\n\tmov.b64 {l4,h4}, p4;\n\tmov.b64 {l5,h5}, p5;\n\t"                   \
-        "mov.b64 {l6,h6}, p6;\n\tmov.b64 {l7,h7}, p7;\n\t"                                            \
-        "add.cc.u32 %0, %0, l0;\n\taddc.cc.u32 %1, %1, h0;\n\taddc.cc.u32 %2, %2, l2;\n\t"           \
-        "addc.cc.u32 %3, %3, h2;\n\taddc.cc.u32 %4, %4, l4;\n\taddc.cc.u32 %5, %5, h4;\n\t"          \
-        "addc.cc.u32 %6, %6, l6;\n\taddc.cc.u32 %7, %7, h6;\n\taddc.u32 %8, %8, 0;\n\t"              \
-        "add.cc.u32 %1, %1, l1;\n\taddc.cc.u32 %2, %2, h1;\n\taddc.cc.u32 %3, %3, l3;\n\t"           \
-        "addc.cc.u32 %4, %4, h3;\n\taddc.cc.u32 %5, %5, l5;\n\taddc.cc.u32 %6, %6, h5;\n\t"          \
-        "addc.cc.u32 %7, %7, l7;\n\taddc.u32 %8, %8, h7;\n\t}"                                       \
-        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),       \
-          "+r"(t[7]), "+r"(t[8])                                                                     \
-        : x0, x1, x2, x3, x4, x5, x6, x7, "r"(y))
+// Montgomery product in two accumulators.  Operand scanning over the words
+// b_i keeps the running value as T = X + Y * 2^32, X holding words of weight
+// 0..7 and Y words of weight 1..8.  Then a_j * b_i lands on an aligned
+// register pair for every j: even j on X words (j, j+1), odd j on Y words
+// (j-1, j).  Each lo/hi multiply-add pair with carry is thus one 64-bit
+// multiply-add on a register pair; when the two halves of a pair straddle a
+// pair boundary (one 9-word accumulator for both parities), the B200 code
+// runs about 130 more instructions per product.
+//
+// Row i adds a * b_i and m * N (m = X_0 * (-N^{-1}) mod 2^32 makes X_0 zero)
+// and divides by 2^32.  After the division X's words sit one weight lower
+// (X_1 at weight 0, X_0 is zero) and Y's words at weights 0..7, so the
+// arrays swap roles: the old Y becomes the new X as it is, and the old X
+// becomes the new Y two words down (old X_{j+2} is new Y_j), except old X_1,
+// which is added into the new X_0.  The two-word move is folded into the
+// next row's odd multiply-add chain.  With inputs below 2N every partial sum
+// stays below 2^288, so no carry leaves either accumulator.
+//
+// The row structure is the even/odd operand-scanning form of the published
+// sppark mont_t multiplication (Supranational, Apache-2.0), which the
+// reference's device_arith2 also uses (core/src/common/mont/src/field.cuh:526-620).
 
-// Montgomery product a*b*R^{-1} mod N in [0, 2N) for inputs in [0, 2N):
-// per row of b, the even/odd wide-product row for a*b[i], the reduction
-// factor m, the even/odd row for m*N, a one-word shift.  No final
-// subtraction (lazy reduction).
+// First row: X = a_even * y, Y = a_odd * y (no accumulation).
+__device__ __forceinline__ void bn_row_first(u32 (&x)[8], u32 (&y)[8], const u32 (&a)[8], u32 w) {
+    asm("mul.lo.u32 %0, %16, %24;\n\tmul.hi.u32 %1, %16, %24;\n\t"
+        "mul.lo.u32 %2, %18, %24;\n\tmul.hi.u32 %3, %18, %24;\n\t"
+        "mul.lo.u32 %4, %20, %24;\n\tmul.hi.u32 %5, %20, %24;\n\t"
+        "mul.lo.u32 %6, %22, %24;\n\tmul.hi.u32 %7, %22, %24;\n\t"
+        "mul.lo.u32 %8, %17, %24;\n\tmul.hi.u32 %9, %17, %24;\n\t"
+        "mul.lo.u32 %10, %19, %24;\n\tmul.hi.u32 %11, %19, %24;\n\t"
+        "mul.lo.u32 %12, %21, %24;\n\tmul.hi.u32 %13, %21, %24;\n\t"
+        "mul.lo.u32 %14, %23, %24;\n\tmul.hi.u32 %15, %23, %24;"
+        : "=r"(x[0]), "=r"(x[1]), "=r"(x[2]), "=r"(x[3]), "=r"(x[4]), "=r"(x[5]), "=r"(x[6]), "=r"(x[7]),
+          "=r"(y[0]), "=r"(y[1]), "=r"(y[2]), "=r"(y[3]), "=r"(y[4]), "=r"(y[5]), "=r"(y[6]), "=r"(y[7])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(w));
+}
+
+// Later row, after the roles swapped: x (the old Y) += old X_1 at weight 0;
+// y (the old X) = old X two words down + a_odd * w; x += a_even * w; the
+// carry out of x (weight 8) into y_7.
+__device__ __forceinline__ void bn_row_next(u32 (&x)[8], u32 (&y)[8], const u32 (&a)[8], u32 w) {
+    asm("add.cc.u32     %0, %0, %9;\n\t"
+        "madc.lo.cc.u32 %8, %17, %24, %10;\n\tmadc.hi.cc.u32 %9, %17, %24, %11;\n\t"
+        "madc.lo.cc.u32 %10, %19, %24, %12;\n\tmadc.hi.cc.u32 %11, %19, %24, %13;\n\t"
+        "madc.lo.cc.u32 %12, %21, %24, %14;\n\tmadc.hi.cc.u32 %13, %21, %24, %15;\n\t"
+        "madc.lo.cc.u32 %14, %23, %24, 0;\n\tmadc.hi.u32    %15, %23, %24, 0;\n\t"
+        "mad.lo.cc.u32  %0, %16, %24, %0;\n\tmadc.hi.cc.u32 %1, %16, %24, %1;\n\t"
+        "madc.lo.cc.u32 %2, %18, %24, %2;\n\tmadc.hi.cc.u32 %3, %18, %24, %3;\n\t"
+        "madc.lo.cc.u32 %4, %20, %24, %4;\n\tmadc.hi.cc.u32 %5, %20, %24, %5;\n\t"
+        "madc.lo.cc.u32 %6, %22, %24, %6;\n\tmadc.hi.cc.u32 %7, %22, %24, %7;\n\t"
+        "addc.u32       %15, %15, 0;"
+        : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]), "+r"(x[7]),
+          "+r"(y[0]), "+r"(y[1]), "+r"(y[2]), "+r"(y[3]), "+r"(y[4]), "+r"(y[5]), "+r"(y[6]), "+r"(y[7])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(w));
+}
+
+// Reduction half of a row: m = x_0 * (-N^{-1}); y += N_odd * m; x += N_even * m
+// (x_0 becomes zero); the carry out of x into y_7.
+template <class F>
+__device__ __forceinline__ void bn_row_reduce(u32 (&x)[8], u32 (&y)[8]) {
+    asm("{\n\t.reg .u32 m;\n\t"
+        "mul.lo.u32     m, %0, %24;\n\t"
+        "mad.lo.cc.u32  %8, m, %17, %8;\n\tmadc.hi.cc.u32 %9, m, %17, %9;\n\t"
+        "madc.lo.cc.u32 %10, m, %19, %10;\n\tmadc.hi.cc.u32 %11, m, %19, %11;\n\t"
+        "madc.lo.cc.u32 %12, m, %21, %12;\n\tmadc.hi.cc.u32 %13, m, %21, %13;\n\t"
+        "madc.lo.cc.u32 %14, m, %23, %14;\n\tmadc.hi.u32    %15, m, %23, %15;\n\t"
+        "mad.lo.cc.u32  %0, m, %16, %0;\n\tmadc.hi.cc.u32 %1, m, %16, %1;\n\t"
+        "madc.lo.cc.u32 %2, m, %18, %2;\n\tmadc.hi.cc.u32 %3, m, %18, %3;\n\t"
+        "madc.lo.cc.u32 %4, m, %20, %4;\n\tmadc.hi.cc.u32 %5, m, %20, %5;\n\t"
+        "madc.lo.cc.u32 %6, m, %22, %6;\n\tmadc.hi.cc.u32 %7, m, %22, %7;\n\t"
+        "addc.u32       %15, %15, 0;\n\t}"
+        : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]), "+r"(x[7]),
+          "+r"(y[0]), "+r"(y[1]), "+r"(y[2]), "+r"(y[3]), "+r"(y[4]), "+r"(y[5]), "+r"(y[6]), "+r"(y[7])
+        : "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5), "n"(F::M6), "n"(F::M7),
+          "n"(F::INV));
+}
+
+// Montgomery product a*b*R^{-1} mod N in [0, 2N) for inputs in [0, 2N).
+// Eight rows with the accumulators alternating; after the last (odd) row the
+// value is u_0..7 + v_1..7 (v_0 is zero).  No final subtraction (lazy
+// reduction).
 template <class F>
 __device__ __forceinline__ Fe<F> fe_mul_inline(const Fe<F> &a, const Fe<F> &b) {
-    u32 t[9];
+    u32 u[8], v[8];
+    bn_row_first(u, v, a.l, b.l[0]);
+    bn_row_reduce<F>(u, v);
 #pragma unroll
-    for (int i = 0; i < 9; i++) t[i] = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-        BN_EO_ROW(t, "r"(a.l[0]), "r"(a.l[1]), "r"(a.l[2]), "r"(a.l[3]), "r"(a.l[4]), "r"(a.l[5]), "r"(a.l[6]),
-                  "r"(a.l[7]), b.l[i]);
-        const u32 m = t[0] * F::INV;
-        BN_EO_ROW(t, "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5), "n"(F::M6),
-                  "n"(F::M7), m);
-#pragma unroll
-        for (int k = 0; k < 8; k++) t[k] = t[k + 1];
-        t[8] = 0;
+    for (int i = 1; i < 8; i += 2) {
+        bn_row_next(v, u, a.l, b.l[i]);
+        bn_row_reduce<F>(v, u);
+        if (i + 1 < 8) {
+            bn_row_next(u, v, a.l, b.l[i + 1]);
+            bn_row_reduce<F>(u, v);
+        }
     }
     Fe<F> r;
-#pragma unroll
-    for (int i = 0; i < 8; i++) r.l[i] = t[i];
+    asm("add.cc.u32  %0, %8, %16;\n\taddc.cc.u32 %1, %9, %17;\n\taddc.cc.u32 %2, %10, %18;\n\t"
+        "addc.cc.u32 %3, %11, %19;\n\taddc.cc.u32 %4, %12, %20;\n\taddc.cc.u32 %5, %13, %21;\n\t"
+        "addc.cc.u32 %6, %14, %22;\n\taddc.u32    %7, %15, 0;"
+        : "=r"(r.l[0]), "=r"(r.l[1]), "=r"(r.l[2]), "=r"(r.l[3]), "=r"(r.l[4]), "=r"(r.l[5]), "=r"(r.l[6]),
+          "=r"(r.l[7])
+        : "r"(u[0]), "r"(u[1]), "r"(u[2]), "r"(u[3]), "r"(u[4]), "r"(u[5]), "r"(u[6]), "r"(u[7]), "r"(v[1]),
+          "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]));
     return r;
 }
 
-// The product is kept out of line: one copy of its ~420 instructions serves
-// every call site.  A mixed addition inlines ten products, and with each
-// inlined the accumulation loop outgrows the instruction cache; measured on
-// B200, the out-of-line product (arguments and result in registers) runs the
-// mixed-addition loop about 20% faster.
+// Inlined: with the carries folded into the multiply-adds a product is about
+// 280 instructions, and ten inlined products per mixed addition leave the
+// scheduler free to interleave independent products.  Measured on B200 this
+// beats an out-of-line product by 13% on the accumulation loop (the
+// out-of-line form won only for the older mul.wide + ALU-add rows, whose
+// inlined copies outgrew the instruction cache).
 template <class F>
-__device__ __noinline__ Fe<F> fe_mul(Fe<F> a, Fe<F> b) {
+__device__ __forceinline__ Fe<F> fe_mul(Fe<F> a, Fe<F> b) {
     return fe_mul_inline<F>(a, b);
 }
 

@@ -202,9 +202,10 @@ cudaError_t impeller_test_field_op(int field, int op, const uint32_t *d_a, const
 cudaError_t impeller_test_point_op(int op, const uint32_t *d_p, const uint32_t *d_q, uint32_t *d_out,
                                    uint64_t count, cudaStream_t s);
 
-/* 32x32 -> 64-bit integer multiply peak of `device`, measured: independent
- * mul.wide.u32 products (the products the Montgomery multiplication is built
- * from), in 10^9 products per second.  Blocks until done. */
+/* Integer-multiply ceiling of `device`, measured: the throughput of
+ * independent Fq Montgomery products (four chains per thread, full
+ * occupancy), in 10^9 32x32 -> 64-bit partial products per second (136 per
+ * Montgomery product).  Blocks until done. */
 cudaError_t impeller_imad_peak(int device, double *gops);
 
 /* Single-thread latency, in SM clock cycles, of a dependent chain of one
