@@ -145,16 +145,51 @@ MULS_PER_MADD = 10
 
 # ------------------------------------------------------------- reference
 
+def reference_gpu(args, n: int, cores: int) -> dict:
+    """The reference's own GPU MSM (core/src/msm/src/msm.cu built unmodified
+    for sm_100a) on the full n-point workload, driven through its msm() C ABI
+    as its Rust operator drives it: pinned host points and scalars, one
+    blocking call per MSM (uploads, kernels, host reduction), wall clock.
+    Inputs come from the CPU oracle's generators; nothing of this library
+    runs here.  Two configurations: MsmConfig::default() and the reference
+    cost model's choice for 2^22."""
+    try:
+        import torch
+        from oracle import ref_gpu as RG
+    except Exception as e:  # pragma: no cover
+        return {"unavailable": f"import failed: {e}"}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    configs = (("default", RG.DEFAULT_CONFIG, 1), ("cost_model_2e22", RG.TUNED_2E22_CONFIG, RG.TUNED_2E22_PARTS))
+    if not all(RG.available(*cfg) for _, cfg, _ in configs):
+        return {"unavailable": "reference sm_100a MSM libraries not built (reference sources absent at build time)"}
+    from oracle import oracle as O
+    pts = O.gen_points(n, seed=0, threads=cores)
+    scal = [O.gen_scalars(n, seed=0, stream=1 + v, threads=cores) for v in range(2)]
+    out = {"n": n, "api": "reference msm() C ABI (core/src/msm/src/msm.h:4-11), sm_100a build of its sources, "
+                          "pinned host buffers, blocking, wall clock", "unit": UNIT}
+    for name, (c, alpha), parts in configs:
+        ref = RG.RefGpuMsm(pts, c, alpha, parts=parts)
+        ms = ref.time_calls(scal, warmup=max(2, args.warmup), steps=args.steps)
+        out[name] = {"window_size": c, "target_window": alpha, "parts": parts, "n_precompute": ref.k,
+                     "ms_per_call": ms, "value": n / (ms / 1e3)}
+        ref.close()
+    return out
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's CPU MSM (the C restatement of
     core/tests/msm_halo2.rs best_multiexp; the Rust original cannot be built
-    here) on the box's host cores, on bounded samples of the 2^22 workload."""
+    here) on the box's host cores, on bounded samples of the 2^22 workload.
+    The line also carries `reference_gpu`: the reference's own sm_100a MSM
+    kernel on the full workload on the same B200."""
     if rank != 0:
         return
     from oracle import oracle as O
     cores = os.cpu_count() or 1
     n_full = 1 << args.log2n
     sample = min(n_full, 1 << 18)
+    gpu_leg = reference_gpu(args, n_full, cores)
     pts = O.gen_points(sample, seed=0, threads=cores)
     scal = [O.gen_scalars(sample, seed=0, stream=1 + v, threads=cores) for v in range(2)]
     for w in range(args.warmup):
@@ -173,6 +208,7 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"2^18-point prefix of the 2^{args.log2n} workload per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": gpu_leg,
     }
     print(json.dumps(line), flush=True)
 
