@@ -31,6 +31,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "BN254 MSM points/s at 2^22; batched vs per-call speedup; p50/p99 latency"
 UNIT = "points/s"
+# kernels of one MSM run: k_zero_words, k_histogram, k_scan_reduce,
+# k_scan_tiles, k_scan_down, k_scatter, k_accumulate, k_fixup_short,
+# k_fixup_long, k_reduce, k_window_sum, k_final
+KERNELS_PER_MSM = 12
 
 
 def env_int(name, default):
@@ -357,7 +361,7 @@ def main():
                        "window_tables_setup_s": round(precompute_s, 3) if c_tab else None,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs > L2: 256 MiB points + 4 rotating 128 MiB scalar vectors"},
-            "gpu_launches": args.steps * 10,
+            "gpu_launches": args.steps * KERNELS_PER_MSM,
             "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
             "roofline": {"bound": "imad", "kernel": "k_accumulate", "achieved": achieved, "peak": peak.value,
                          "unit": "G 32x32->64 products/s", "frac": achieved / peak.value,
@@ -515,7 +519,7 @@ def batched_vs_per_call(M, ctx, dev, args) -> dict:
             "total_points": total, "batched_ms": tb, "per_call_ms": tp,
             "batched_points_per_s": total / (tb * 1e-3), "per_call_points_per_s": total / (tp * 1e-3),
             "speedup": tp / tb, "results_identical": same, "launches_per_batch": launches,
-            "launches_per_call_total": 10 * len(sizes)}
+            "launches_per_call_total": KERNELS_PER_MSM * len(sizes)}
 
 
 if __name__ == "__main__":

@@ -15,6 +15,17 @@
 //     Montgomery form, identity (0,0) (msm.cu:37-39).
 // Unlike the reference, the per-part and per-card partial sums are added on
 // the device, and only the canonical affine result leaves the GPU.
+//
+// Uploads stream: a card's points and scalars are copied in chunks on a copy
+// stream while the previous chunk is sorted and accumulated on the compute
+// stream; every chunk adds its bucket sums into the card's accumulators and
+// the bucket reduction runs once per batch group, as the reference
+// accumulates all parts into one bucket set before reducing
+// (msm_impl.cuh:384-575).  With parts == 1 the whole card range stays
+// resident (later batch groups reuse the points) and is streamed in chunks
+// of about 2^20 points; with parts > 1 each part is a chunk, double-buffered
+// in two stages (the reference's stage_scalers / stage_points = 2 that
+// get_best_config pairs with parts > 1, core/src/msm.rs:89).
 #include <algorithm>
 #include <cstdio>
 #include <map>
@@ -67,8 +78,19 @@ bool make_config(unsigned window_size, unsigned target_window, int debug, Config
 // Per-card carve-out of the caller's buffer.
 struct CardLayout {
     u64 card_off = 0, card_len = 0, part_len = 0;
-    size_t o_points = 0, o_scalars = 0, o_carry = 0, o_results = 0, o_combine = 0, o_plan = 0, bytes = 0;
+    size_t o_points = 0, o_scalars = 0, o_carry = 0, o_results = 0, o_combine = 0, o_plan = 0, o_acc = 0;
+    size_t o_images = 0, image_cap = 0, bytes = 0;  // streamed: one table image per chunk
 };
+
+// Chunks a resident (parts == 1) range of `len` points streams in: 1 (no
+// streaming) below 2^21 points, else about 2^20 points per chunk, at most 8.
+u32 stream_chunks(u64 len) {
+    const u64 k = len >> 20;
+    return k < 2 ? 1u : (u32)std::min<u64>(k, 8);
+}
+
+// parts > 1: each part is a chunk, in one of two buffer stages.
+constexpr u32 PART_STAGES = 2;
 
 std::vector<MsmShape> group_shapes(const Config &cfg, u32 M, u32 n, u32 part_len) {
     std::vector<MsmShape> s(M, MsmShape{n, cfg.c, cfg.n_windows, part_len, 0});
@@ -86,38 +108,65 @@ bool card_layout(const Config &cfg, int device, u64 len, u32 num_cards, u32 card
         return false;
     }
     plan_bytes = 0;
+    size_t acc_bytes = 0, images = 0;
     if (L.part_len) {
         Plan p;
         if (!Plan::build(p, device, group_shapes(cfg, batch_per_run, (u32)L.part_len, (u32)L.part_len))) return false;
         plan_bytes = p.scratch_bytes();
+        const u64 nchunks = parts > 1 ? (L.card_len + L.part_len - 1) / L.part_len : stream_chunks(L.card_len);
+        if (nchunks > 1) {
+            acc_bytes = p.acc_bytes();
+            L.image_cap = align_up(p.image_bytes(), 256);
+            images = nchunks * L.image_cap;
+        }
     }
+    const size_t stages = parts > 1 ? PART_STAGES : 1;
     size_t off = 0;
     auto take = [&](size_t b) {
         size_t o = off;
         off = align_up(off + b, 256);
         return o;
     };
-    L.o_points = take((size_t)cfg.n_tables * L.part_len * 64);
-    L.o_scalars = take((size_t)batch_per_run * L.part_len * 32);
+    L.o_points = take(stages * cfg.n_tables * L.part_len * 64);
+    L.o_scalars = take(stages * batch_per_run * L.part_len * 32);
     L.o_carry = take((size_t)batch_per_run * 128);
     L.o_results = take((size_t)batch_per_run * 64);
     L.o_combine = take((size_t)num_cards * 128 + 64);
     L.o_plan = take(plan_bytes);
+    L.o_acc = take(acc_bytes);
+    L.o_images = take(images);
     L.bytes = off;
     return true;
 }
 
-cudaStream_t device_stream(int device) {
+// One compute stream (role 0) and one copy stream (role 1) per device, kept
+// for the life of the process.
+cudaStream_t device_stream(int device, int role = 0) {
     static std::mutex mu;
-    static std::map<int, cudaStream_t> streams;
+    static std::map<std::pair<int, int>, cudaStream_t> streams;
     std::lock_guard<std::mutex> g(mu);
-    auto it = streams.find(device);
+    auto key = std::make_pair(device, role);
+    auto it = streams.find(key);
     if (it != streams.end()) return it->second;
     cudaStream_t s = nullptr;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
-    streams[device] = s;
+    streams[key] = s;
     return s;
 }
+
+// Events of one streamed call, destroyed with it.
+struct EventPool {
+    std::vector<cudaEvent_t> ev;
+    cudaEvent_t get() {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+        ev.push_back(e);
+        return e;
+    }
+    ~EventPool() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+};
 
 struct CardJob {
     const Config *cfg;
@@ -133,11 +182,50 @@ struct CardJob {
     std::string error;
 };
 
+// Plans persist per device across calls (their pinned table images and
+// events are the costly part to create); calls on one device are serialized.
+struct DevicePlans {
+    std::mutex mu;
+    std::map<std::vector<u32>, std::unique_ptr<Plan>> plans;
+    std::vector<std::vector<u32>> order;  // oldest first
+    void *host_images = nullptr;          // pinned: the chunk table images of one call
+    size_t host_images_cap = 0;
+};
+
+DevicePlans &device_plans(int device) {
+    static std::mutex mu;
+    static std::map<int, std::unique_ptr<DevicePlans>> all;
+    std::lock_guard<std::mutex> g(mu);
+    auto &p = all[device];
+    if (!p) p.reset(new DevicePlans());
+    return *p;
+}
+
+constexpr size_t PLAN_CACHE_CAP = 32;
+
+Plan *cached_plan(DevicePlans &D, int device, const Config &cfg, u32 M, u32 n, u32 stride) {
+    std::vector<u32> key{cfg.c, cfg.n_windows, M, n, stride};
+    auto it = D.plans.find(key);
+    if (it != D.plans.end()) return it->second.get();
+    if (D.plans.size() >= PLAN_CACHE_CAP) {
+        D.plans.erase(D.order.front());  // the oldest: not used by the current call
+        D.order.erase(D.order.begin());
+    }
+    std::unique_ptr<Plan> p(new Plan());
+    if (!Plan::build(*p, device, group_shapes(cfg, M, n, stride))) return nullptr;
+    Plan *raw = p.get();
+    D.plans[key] = std::move(p);
+    D.order.push_back(key);
+    return raw;
+}
+
 cudaError_t run_card(CardJob &J) {
     const Config &cfg = *J.cfg;
     CK(cudaSetDevice(J.device));
-    cudaStream_t st = device_stream(J.device);
-    if (!st) {
+    DevicePlans &D = device_plans(J.device);
+    std::lock_guard<std::mutex> hold(D.mu);
+    cudaStream_t st = device_stream(J.device, 0), cs = device_stream(J.device, 1);
+    if (!st || !cs) {
         set_error("could not create a stream");
         return cudaErrorUnknown;
     }
@@ -146,71 +234,155 @@ cudaError_t run_card(CardJob &J) {
     u32 *d_scalars = reinterpret_cast<u32 *>(base + J.L.o_scalars);
     u32 *d_carry = reinterpret_cast<u32 *>(base + J.L.o_carry);
     u32 *d_results = reinterpret_cast<u32 *>(base + J.L.o_results);
+    u32 *d_acc = reinterpret_cast<u32 *>(base + J.L.o_acc);
     void *plan_scratch = base + J.L.o_plan;
     const bool multi = J.num_cards > 1;
     if (multi) J.partials.assign((size_t)J.batches * 32, 0);
+    const u64 part_len = J.L.part_len, card_len = J.L.card_len;
+    const bool staged = J.parts > 1;
+    const u32 stride = (u32)part_len;  // distance between window tables in a points buffer
+    const size_t point_stage = (size_t)cfg.n_tables * part_len * 16;  // u32 per stage
+    EventPool events;
 
-    std::map<std::pair<u32, u32>, std::unique_ptr<Plan>> plans;
-    auto get_plan = [&](u32 M, u32 n) -> Plan * {
-        auto key = std::make_pair(M, n);
-        auto it = plans.find(key);
-        if (it != plans.end()) return it->second.get();
-        std::unique_ptr<Plan> p(new Plan());
-        if (!Plan::build(*p, J.device, group_shapes(cfg, M, n, (u32)J.L.part_len))) return nullptr;
-        Plan *raw = p.get();
-        plans[key] = std::move(p);
-        return raw;
-    };
+    // chunk k covers points [k * chunk, ...) of the card range
+    const u64 chunk = staged ? part_len : (card_len + stream_chunks(card_len) - 1) / stream_chunks(card_len);
+    const u32 nchunks = card_len ? (u32)((card_len + chunk - 1) / chunk) : 0;
 
     bool points_resident = false;
     for (u32 g = 0; g < J.batches; g += J.batch_per_run) {
         const u32 M = std::min(J.batch_per_run, J.batches - g);
-        if (J.L.card_len == 0) {
+        if (card_len == 0) {
             // an empty range contributes the identity
             if (!multi)
                 for (u32 b = 0; b < M; b++) std::fill(J.h_result[g + b], J.h_result[g + b] + 16, 0u);
             continue;
         }
-        CK(cudaMemsetAsync(d_carry, 0, (size_t)M * 128, st));
-        for (u32 p = 0; p < J.parts; p++) {
-            const u64 off = (u64)p * J.L.part_len;
-            if (off >= J.L.card_len) break;
-            const u64 cur = std::min<u64>(J.L.part_len, J.L.card_len - off);
-            const bool last = off + cur >= J.L.card_len;
-            if (!(points_resident && J.parts == 1)) {
+        const int mode = multi ? 2 : 0;
+        if (multi) CK(cudaMemsetAsync(d_carry, 0, (size_t)M * 128, st));
+        const size_t scalar_stage = (size_t)M * part_len * 8;  // u32 per stage
+        cudaEvent_t t0 = nullptr, t1 = nullptr;
+        if (cfg.debug) {
+            cudaEventCreate(&t0);
+            cudaEventCreate(&t1);
+            cudaEventRecord(t0, st);
+        }
+        if (nchunks == 1) {
+            // one chunk: upload, then the plain run
+            if (!points_resident)
                 for (u32 t = 0; t < cfg.n_tables; t++)
-                    CK(cudaMemcpyAsync(d_points + (size_t)t * J.L.part_len * 16,
-                                       J.h_points[t] + (J.L.card_off + off) * 16, cur * 64, cudaMemcpyHostToDevice,
-                                       st));
-                points_resident = true;
-            }
+                    CK(cudaMemcpyAsync(d_points + (size_t)t * part_len * 16, J.h_points[t] + J.L.card_off * 16,
+                                       card_len * 64, cudaMemcpyHostToDevice, st));
+            points_resident = !staged;
             std::vector<const u32 *> sc(M);
             for (u32 b = 0; b < M; b++) {
-                CK(cudaMemcpyAsync(d_scalars + (size_t)b * J.L.part_len * 8, J.h_scalars[g + b] + (J.L.card_off + off) * 8,
-                                   cur * 32, cudaMemcpyHostToDevice, st));
-                sc[b] = d_scalars + (size_t)b * J.L.part_len * 8;
+                u32 *dst = d_scalars + (size_t)b * part_len * 8;
+                CK(cudaMemcpyAsync(dst, J.h_scalars[g + b] + J.L.card_off * 8, card_len * 32,
+                                   cudaMemcpyHostToDevice, st));
+                sc[b] = dst;
             }
-            Plan *plan = get_plan(M, (u32)cur);
+            Plan *plan = cached_plan(D, J.device, cfg, M, (u32)card_len, stride);
             if (!plan) return cudaErrorInvalidValue;
-            const int mode = (last && !multi) ? 1 : 2;
-            cudaEvent_t t0 = nullptr, t1 = nullptr;
-            if (cfg.debug) {
-                cudaEventCreate(&t0);
-                cudaEventCreate(&t1);
-                cudaEventRecord(t0, st);
-            }
             cudaError_t e = plan->enqueue(plan_scratch, d_points, sc.data(), d_results, mode, st, d_carry);
             if (e != cudaSuccess) return e;
-            if (cfg.debug) {
-                cudaEventRecord(t1, st);
-                cudaEventSynchronize(t1);
-                float ms = 0;
-                cudaEventElapsedTime(&ms, t0, t1);
-                std::fprintf(stderr, "impeller msm: card %d group %u part %u n=%llu batch=%u: %.3f ms\n", J.device, g,
-                             p, (unsigned long long)cur, M, ms);
-                cudaEventDestroy(t0);
-                cudaEventDestroy(t1);
+        } else {
+            // streamed: copies on cs, chunk k's compute on st once its data landed
+            cudaEvent_t free_ev = events.get();
+            if (!free_ev) return cudaErrorUnknown;
+            CK(cudaEventRecord(free_ev, st));  // earlier work on st may still read the buffers
+            CK(cudaStreamWaitEvent(cs, free_ev, 0));
+            // every chunk's table image, written on the host and uploaded in one
+            // copy ahead of the data (the previous call's copy has completed)
+            const size_t img_bytes = (size_t)nchunks * J.L.image_cap;
+            if (D.host_images_cap < img_bytes) {
+                if (D.host_images) cudaFreeHost(D.host_images);
+                D.host_images = nullptr;
+                D.host_images_cap = 0;
+                CK(cudaHostAlloc(&D.host_images, img_bytes, cudaHostAllocPortable));
+                D.host_images_cap = img_bytes;
             }
+            std::vector<Plan *> chunk_plan(nchunks, nullptr);
+            for (u32 k = 0; k < nchunks; k++) {
+                const u64 s0 = (u64)k * chunk;
+                const u64 mk = std::min<u64>(chunk, card_len - s0);
+                const u32 slot = staged ? k % PART_STAGES : 0;
+                std::vector<const u32 *> sc(M);
+                for (u32 b = 0; b < M; b++)
+                    sc[b] = staged ? d_scalars + slot * scalar_stage + (size_t)b * part_len * 8
+                                   : d_scalars + (size_t)b * part_len * 8 + s0 * 8;
+                chunk_plan[k] = cached_plan(D, J.device, cfg, M, (u32)mk, stride);
+                if (!chunk_plan[k]) return cudaErrorInvalidValue;
+                if (chunk_plan[k]->image_bytes() > J.L.image_cap) {
+                    set_error("msm: chunk table image exceeds its slot");
+                    return cudaErrorInvalidValue;
+                }
+                chunk_plan[k]->write_image(static_cast<unsigned char *>(D.host_images) + k * J.L.image_cap, sc.data());
+            }
+            unsigned char *d_images = base + J.L.o_images;
+            CK(cudaMemcpyAsync(d_images, D.host_images, img_bytes, cudaMemcpyHostToDevice, cs));
+            std::vector<cudaEvent_t> computed(nchunks, nullptr);
+            // debug: timing events per chunk (data landed, compute start, compute end)
+            std::vector<cudaEvent_t> tl(cfg.debug ? 3 * nchunks : 0, nullptr);
+            for (auto &e : tl) cudaEventCreate(&e);
+            Plan *plan = nullptr;
+            for (u32 k = 0; k < nchunks; k++) {
+                const u64 s0 = (u64)k * chunk;
+                const u64 mk = std::min<u64>(chunk, card_len - s0);
+                const u32 slot = staged ? k % PART_STAGES : 0;
+                if (staged && k >= PART_STAGES) CK(cudaStreamWaitEvent(cs, computed[k - PART_STAGES], 0));
+                // points of this chunk: staged -> its stage buffer; resident -> in place
+                u32 *pbase = staged ? d_points + slot * point_stage : d_points + s0 * 16;
+                if (!points_resident)
+                    for (u32 t = 0; t < cfg.n_tables; t++)
+                        CK(cudaMemcpyAsync(pbase + (size_t)t * part_len * 16,
+                                           J.h_points[t] + (J.L.card_off + s0) * 16, mk * 64,
+                                           cudaMemcpyHostToDevice, cs));
+                for (u32 b = 0; b < M; b++) {
+                    u32 *dst = staged ? d_scalars + slot * scalar_stage + (size_t)b * part_len * 8
+                                      : d_scalars + (size_t)b * part_len * 8 + s0 * 8;
+                    CK(cudaMemcpyAsync(dst, J.h_scalars[g + b] + (J.L.card_off + s0) * 8, mk * 32,
+                                       cudaMemcpyHostToDevice, cs));
+                }
+                cudaEvent_t landed = events.get();
+                if (!landed) return cudaErrorUnknown;
+                CK(cudaEventRecord(landed, cs));
+                if (cfg.debug) cudaEventRecord(tl[3 * k], cs);
+                CK(cudaStreamWaitEvent(st, landed, 0));
+                if (cfg.debug) cudaEventRecord(tl[3 * k + 1], st);
+                plan = chunk_plan[k];
+                cudaError_t e = plan->launch_chunk(plan_scratch, pbase, d_acc, k == 0, st, d_images + k * J.L.image_cap);
+                if (e != cudaSuccess) return e;
+                if (cfg.debug) cudaEventRecord(tl[3 * k + 2], st);
+                if (staged) {
+                    computed[k] = events.get();
+                    if (!computed[k]) return cudaErrorUnknown;
+                    CK(cudaEventRecord(computed[k], st));
+                }
+            }
+            points_resident = !staged;
+            cudaError_t e = plan->launch_chunked_tail(plan_scratch, d_acc, d_results, mode, st, d_carry,
+                                                      d_images + (size_t)(nchunks - 1) * J.L.image_cap);
+            if (e != cudaSuccess) return e;
+            if (cfg.debug) {
+                cudaStreamSynchronize(st);
+                for (u32 k = 0; k < nchunks; k++) {
+                    float a = 0, b = 0, c = 0;
+                    cudaEventElapsedTime(&a, t0, tl[3 * k]);
+                    cudaEventElapsedTime(&b, t0, tl[3 * k + 1]);
+                    cudaEventElapsedTime(&c, t0, tl[3 * k + 2]);
+                    std::fprintf(stderr, "impeller msm:   chunk %u: landed %.3f ms, compute %.3f .. %.3f ms\n", k, a, b, c);
+                }
+                for (auto &ev : tl) cudaEventDestroy(ev);
+            }
+        }
+        if (cfg.debug) {
+            cudaEventRecord(t1, st);
+            cudaEventSynchronize(t1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, t0, t1);
+            std::fprintf(stderr, "impeller msm: card %d group %u n=%llu batch=%u chunks=%u: %.3f ms\n", J.device, g,
+                         (unsigned long long)card_len, M, nchunks, ms);
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
         }
         if (!multi) {
             for (u32 b = 0; b < M; b++)

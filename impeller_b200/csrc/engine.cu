@@ -191,7 +191,7 @@ Plan::~Plan() {
         for (auto e : set) cudaEventDestroy(e);
 }
 
-u32 Plan::launches() const { return 11; }
+u32 Plan::launches() const { return 12; }
 
 const char *Plan::phase_name(int i) {
     static const char *names[NPHASE] = {"tables", "histogram", "scan", "scatter",
@@ -251,80 +251,153 @@ cudaError_t Plan::mark_staged(cudaStream_t st) {
     return cudaSuccess;
 }
 
-cudaError_t Plan::launch(void *scratch, const u32 *points, u32 *results, int carry_mode, cudaStream_t st,
-                         u32 *carry_ext, bool record_staged) {
-    unsigned char *s = static_cast<unsigned char *>(scratch);
-    const MsmDesc *d_desc = reinterpret_cast<const MsmDesc *>(s + layout.o_tables + desc_off);
-    const WinDesc *d_wins = reinterpret_cast<const WinDesc *>(s + layout.o_tables + win_off);
-    const uint2 *d_blk = reinterpret_cast<const uint2 *>(s + layout.o_tables + blk_off);
-    u32 *counts = reinterpret_cast<u32 *>(s + layout.o_counts);
-    u32 *cursor = reinterpret_cast<u32 *>(s + layout.o_cursor);
-    u32 *offsets = reinterpret_cast<u32 *>(s + layout.o_offsets);
-    u32 *tiles = reinterpret_cast<u32 *>(s + layout.o_tiles);
-    u32 *entries = reinterpret_cast<u32 *>(s + layout.o_entries);
-    u32 *buckets = reinterpret_cast<u32 *>(s + layout.o_buckets);
-    u32 *recb = reinterpret_cast<u32 *>(s + layout.o_recb);
-    u32 *recp = reinterpret_cast<u32 *>(s + layout.o_recp);
-    u32 *parts = reinterpret_cast<u32 *>(s + layout.o_parts);
-    u32 *parts_s = reinterpret_cast<u32 *>(s + layout.o_parts_s);
-    u32 *wres = reinterpret_cast<u32 *>(s + layout.o_wres);
-    u32 *longl = reinterpret_cast<u32 *>(s + layout.o_long);
-    u32 *carry = carry_ext ? carry_ext : reinterpret_cast<u32 *>(s + layout.o_carry);
-    u32 *res = results ? results : reinterpret_cast<u32 *>(s + layout.o_results);
+// Scratch pointers of one plan.
+struct PlanPtrs {
+    const MsmDesc *desc;
+    const WinDesc *wins;
+    const uint2 *blk;
+    u32 *counts, *cursor, *offsets, *tiles, *entries, *buckets, *recb, *recp, *parts, *parts_s, *wres, *longl;
+    u32 *carry, *res;
+};
 
-    cudaError_t pe;
+static PlanPtrs plan_ptrs(const PlanLayout &L, size_t desc_off, size_t win_off, size_t blk_off, void *scratch,
+                          u32 *carry_ext, u32 *results, const void *d_image = nullptr) {
+    unsigned char *s = static_cast<unsigned char *>(scratch);
+    const unsigned char *img = d_image ? static_cast<const unsigned char *>(d_image) : s + L.o_tables;
+    PlanPtrs p;
+    p.desc = reinterpret_cast<const MsmDesc *>(img + desc_off);
+    p.wins = reinterpret_cast<const WinDesc *>(img + win_off);
+    p.blk = reinterpret_cast<const uint2 *>(img + blk_off);
+    p.counts = reinterpret_cast<u32 *>(s + L.o_counts);
+    p.cursor = reinterpret_cast<u32 *>(s + L.o_cursor);
+    p.offsets = reinterpret_cast<u32 *>(s + L.o_offsets);
+    p.tiles = reinterpret_cast<u32 *>(s + L.o_tiles);
+    p.entries = reinterpret_cast<u32 *>(s + L.o_entries);
+    p.buckets = reinterpret_cast<u32 *>(s + L.o_buckets);
+    p.recb = reinterpret_cast<u32 *>(s + L.o_recb);
+    p.recp = reinterpret_cast<u32 *>(s + L.o_recp);
+    p.parts = reinterpret_cast<u32 *>(s + L.o_parts);
+    p.parts_s = reinterpret_cast<u32 *>(s + L.o_parts_s);
+    p.wres = reinterpret_cast<u32 *>(s + L.o_wres);
+    p.longl = reinterpret_cast<u32 *>(s + L.o_long);
+    p.carry = carry_ext ? carry_ext : reinterpret_cast<u32 *>(s + L.o_carry);
+    p.res = results ? results : reinterpret_cast<u32 *>(s + L.o_results);
+    return p;
+}
+
 #define MARK(k)                                  \
     if ((pe = prof_mark((k), st)) != cudaSuccess) \
         return pe;
+
+// Zero n words at p and m words at q.
+__global__ void k_zero_words(u32 *__restrict__ p, u32 n, u32 *__restrict__ q, u32 m) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0;
+    if (blockIdx.x == 0 && threadIdx.x < m) q[threadIdx.x] = 0;
+}
+
+// Table image upload (unless the image is already on the device at
+// d_image), counting sort, accumulation and fixups: every bucket with
+// entries holds its sum in `buckets`.  No copy or memset runs on the stream
+// when d_image is given, so nothing here queues behind transfers on a copy
+// engine.
+cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, bool record_staged,
+                            const void *d_image) {
+    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, scratch, nullptr, nullptr, d_image);
+    cudaError_t pe;
     MARK(0);
-    CK(cudaMemcpyAsync(s + layout.o_tables, staging, tables.size(), cudaMemcpyHostToDevice, st));
-    if (record_staged) CK(cudaEventRecord(staged, st));
-    CK(cudaMemsetAsync(counts, 0, (size_t)nb_pad * 4, st));
+    if (!d_image) {
+        CK(cudaMemcpyAsync(static_cast<unsigned char *>(scratch) + layout.o_tables, staging, tables.size(),
+                           cudaMemcpyHostToDevice, st));
+        if (record_staged) CK(cudaEventRecord(staged, st));
+    }
+    // the bucket counts and the long-run counter of the fixups
+    k_zero_words<<<std::max(1u, std::min((nb_pad + 255) / 256, (u32)sm_count(device) * 4)), 256, 0, st>>>(
+        p.counts, nb_pad, p.longl, 1);
+    CK_LAUNCH("k_zero_words");
     MARK(1);
 
     dim3 hgrid(hist_grid_x, M);
-    k_histogram<<<hgrid, 256, 0, st>>>(d_desc, counts);
+    k_histogram<<<hgrid, 256, 0, st>>>(p.desc, p.counts);
     CK_LAUNCH("k_histogram");
     MARK(2);
-    k_scan_reduce<<<ntiles, SCAN_BLOCK, 0, st>>>(counts, tiles);
+    k_scan_reduce<<<ntiles, SCAN_BLOCK, 0, st>>>(p.counts, p.tiles);
     CK_LAUNCH("k_scan_reduce");
-    k_scan_tiles<<<1, SCAN_BLOCK, 0, st>>>(tiles, ntiles);
+    k_scan_tiles<<<1, SCAN_BLOCK, 0, st>>>(p.tiles, ntiles);
     CK_LAUNCH("k_scan_tiles");
-    k_scan_down<<<ntiles, SCAN_BLOCK, 0, st>>>(counts, tiles, offsets, cursor, nb, ntiles);
+    k_scan_down<<<ntiles, SCAN_BLOCK, 0, st>>>(p.counts, p.tiles, p.offsets, p.cursor, nb, ntiles);
     CK_LAUNCH("k_scan_down");
     MARK(3);
-    k_scatter<<<hgrid, 256, 0, st>>>(d_desc, cursor, entries);
+    k_scatter<<<hgrid, 256, 0, st>>>(p.desc, p.cursor, p.entries);
     CK_LAUNCH("k_scatter");
     MARK(4);
 
-    AccumArgs aa{entries, offsets, nb, points, buckets, recb, recp};
+    AccumArgs aa{p.entries, p.offsets, nb, points, p.buckets, p.recb, p.recp};
     k_accumulate<<<accum_blocks, accum_block, 0, st>>>(aa);
     CK_LAUNCH("k_accumulate");
     MARK(5);
 
     const u32 T = accum_blocks * accum_block;
-    CK(cudaMemsetAsync(longl, 0, 4, st));
-    FixupArgs fa{offsets, nb, T, recb, recp, buckets, longl, long_cap};
+    FixupArgs fa{p.offsets, nb, T, p.recb, p.recp, p.buckets, p.longl, long_cap};
     k_fixup_short<<<(T + 255) / 256, 256, 0, st>>>(fa);
     CK_LAUNCH("k_fixup_short");
     k_fixup_long<<<(u32)sm_count(device), 256, 0, st>>>(fa);
     CK_LAUNCH("k_fixup_long");
     MARK(6);
+    return cudaSuccess;
+}
 
-    ReduceArgs ra{d_wins, d_blk, offsets, buckets, parts, parts_s};
+// Bucket reduction, window sums, Horner combine and affine output, over
+// `buckets` (the plan's own, sparse by offsets, or dense accumulators).
+cudaError_t Plan::run_tail(void *scratch, const u32 *buckets, bool dense, u32 *results, int carry_mode,
+                           cudaStream_t st, u32 *carry_ext, const void *d_image) {
+    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, scratch, carry_ext, results, d_image);
+    cudaError_t pe;
+    ReduceArgs ra{p.wins, p.blk, p.offsets, buckets, p.parts, p.parts_s, dense ? 1u : 0u};
     k_reduce<<<nrblocks, REDUCE_BLOCK, 0, st>>>(ra);
     CK_LAUNCH("k_reduce");
     MARK(7);
 
-    WindowSumArgs wa{d_desc, d_wins, parts, parts_s, nwins, wres};
+    WindowSumArgs wa{p.desc, p.wins, p.parts, p.parts_s, nwins, p.wres};
     k_window_sum<<<nwins, WSUM_BLOCK, 0, st>>>(wa);
     CK_LAUNCH("k_window_sum");
-    FinalArgs fa2{d_desc, wres, M, carry_mode == 0 ? nullptr : carry, carry_mode == 2 ? 0 : 1, res};
+    FinalArgs fa2{p.desc, p.wres, M, carry_mode == 0 ? nullptr : p.carry, carry_mode == 2 ? 0 : 1, p.res};
     k_final<<<(M + 31) / 32, 32, 0, st>>>(fa2);
     CK_LAUNCH("k_final");
     MARK(8);
-#undef MARK
     return cudaSuccess;
+}
+#undef MARK
+
+cudaError_t Plan::launch(void *scratch, const u32 *points, u32 *results, int carry_mode, cudaStream_t st,
+                         u32 *carry_ext, bool record_staged) {
+    cudaError_t e = run_front(scratch, points, st, record_staged, nullptr);
+    if (e != cudaSuccess) return e;
+    const u32 *buckets = reinterpret_cast<const u32 *>(static_cast<unsigned char *>(scratch) + layout.o_buckets);
+    return run_tail(scratch, buckets, false, results, carry_mode, st, carry_ext, nullptr);
+}
+
+size_t Plan::image_bytes() const { return tables.size(); }
+
+void Plan::write_image(void *dst, const u32 *const *scalars) const {
+    std::memcpy(dst, tables.data(), tables.size());
+    MsmDesc *d = reinterpret_cast<MsmDesc *>(static_cast<unsigned char *>(dst) + desc_off);
+    for (u32 m = 0; m < M; m++) d[m].scalars = scalars[m];
+}
+
+cudaError_t Plan::launch_chunk(void *scratch, const u32 *points, u32 *acc, bool first, cudaStream_t st,
+                               const void *d_image) {
+    cudaError_t e = run_front(scratch, points, st, true, d_image);
+    if (e != cudaSuccess) return e;
+    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, scratch, nullptr, nullptr, d_image);
+    const u32 blocks = std::max(1u, std::min((nb + 255) / 256, (u32)sm_count(device) * 8));
+    k_bucket_merge<<<blocks, 256, 0, st>>>(p.offsets, p.buckets, acc, nb, first ? 1u : 0u);
+    CK_LAUNCH("k_bucket_merge");
+    return cudaSuccess;
+}
+
+cudaError_t Plan::launch_chunked_tail(void *scratch, const u32 *acc, u32 *results, int carry_mode, cudaStream_t st,
+                                      u32 *carry_ext, const void *d_image) {
+    return run_tail(scratch, acc, true, results, carry_mode, st, carry_ext, d_image);
 }
 
 cudaError_t Plan::enqueue(void *scratch, const u32 *points, const u32 *const *scalars, u32 *results, int carry_mode,

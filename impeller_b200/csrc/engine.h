@@ -76,6 +76,24 @@ class Plan {
                        u32 *carry_ext = nullptr, bool record_staged = true);
     cudaError_t mark_staged(cudaStream_t stream);
 
+    // Streamed accumulation, for points that arrive in chunks: each chunk
+    // (this plan's MSMs over the chunk's points and scalars) sorts and
+    // accumulates, then adds its bucket sums into `acc` (nb XYZZ,
+    // caller-owned; first = overwrite).  launch_chunked_tail reduces `acc`
+    // and emits results as launch does.  Every plan used on one `acc` must
+    // have the same window structure (same c, windows and MSM count).
+    // d_image: the chunk's table image (write_image) already on the device;
+    // null = stage() before and upload on the stream as launch does.
+    cudaError_t launch_chunk(void *scratch, const u32 *points, u32 *acc, bool first, cudaStream_t stream,
+                             const void *d_image = nullptr);
+    cudaError_t launch_chunked_tail(void *scratch, const u32 *acc, u32 *results, int carry_mode,
+                                    cudaStream_t stream, u32 *carry_ext = nullptr, const void *d_image = nullptr);
+    size_t acc_bytes() const { return (size_t)nb * 128; }
+    // The table image (descriptors with these scalar pointers, windows,
+    // reduce blocks) as launch uploads it, written to host memory at dst.
+    size_t image_bytes() const;
+    void write_image(void *dst, const u32 *const *scalars) const;
+
     size_t scratch_bytes() const { return layout.bytes; }
     u32 launches() const;
     u32 *carry_ptr(void *scratch) const;
@@ -103,6 +121,11 @@ class Plan {
     Plan &operator=(const Plan &) = delete;
 
   private:
+    cudaError_t run_front(void *scratch, const u32 *points, cudaStream_t stream, bool record_staged,
+                          const void *d_image);
+    cudaError_t run_tail(void *scratch, const u32 *buckets, bool dense, u32 *results, int carry_mode,
+                         cudaStream_t stream, u32 *carry_ext, const void *d_image);
+
     void *staging = nullptr;     // pinned copy of the tables
     void *ext_staging = nullptr; // caller-owned staging (set_staging)
     size_t ext_cap = 0;

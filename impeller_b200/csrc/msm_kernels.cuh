@@ -386,6 +386,23 @@ __global__ void k_fixup_long(FixupArgs f) {
     }
 }
 
+// Streamed accumulation: an MSM whose points arrive in chunks runs the
+// sort and the accumulation per chunk and adds each chunk's bucket sums into
+// persistent accumulators `acc` (nb XYZZ); the reduction runs once, over
+// `acc` (dense).  first: acc = this chunk's sums (identity where empty).
+__global__ void k_bucket_merge(const u32 *__restrict__ offsets, const u32 *__restrict__ buckets,
+                               u32 *__restrict__ acc, u32 nb, u32 first) {
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
+        const bool filled = offsets[g + 1] != offsets[g];
+        if (first) {
+            xyzz_store(acc + (size_t)g * 32, filled ? xyzz_load(buckets + (size_t)g * 32) : xyzz_identity());
+        } else if (filled) {
+            xyzz_store(acc + (size_t)g * 32,
+                       xyzz_add(xyzz_load(acc + (size_t)g * 32), xyzz_load(buckets + (size_t)g * 32)));
+        }
+    }
+}
+
 // ----------------------------------------------------------------- reduce
 //
 // Window total T = sum_{k=1..B} k * S_k.  Lane j of a window owns the weights
@@ -406,6 +423,7 @@ struct ReduceArgs {
     const u32 *buckets;
     u32 *parts_v;         // XYZZ per reduce warp
     u32 *parts_s;         // XYZZ per reduce warp
+    u32 dense;            // 1: every bucket holds a point (identity when empty); ignore offsets
 };
 
 static constexpr u32 REDUCE_BLOCK = 128;
@@ -424,7 +442,7 @@ __global__ void __launch_bounds__(REDUCE_BLOCK, 3) k_reduce(ReduceArgs r) {
         const u32 hi = min(lo + wd.chunk, wd.nbuckets);
         for (u32 k = hi; k > lo; k--) {
             const u32 g = wd.bucket_base + k - 1;
-            if (r.offsets[g + 1] != r.offsets[g]) sum = xyzz_add(sum, xyzz_load(r.buckets + (size_t)g * 32));
+            if (r.dense || r.offsets[g + 1] != r.offsets[g]) sum = xyzz_add(sum, xyzz_load(r.buckets + (size_t)g * 32));
             sos = xyzz_add(sos, sum);
         }
     }

@@ -293,6 +293,61 @@ def test_reference_abi_precompute_tables(M):
     del keep
 
 
+def test_reference_abi_streamed_chunks(M):
+    # parts of >= 2^21 points stream their upload in chunks; uneven chunk
+    # sizes, two batch groups (the second with resident points), the oracle
+    # on one output and the resident-SRS path on all
+    n = (1 << 21) + 4321
+    d = M.gen_points_device(n, seed=14)
+    pts = M.to_host(d).reshape(n, 16)
+    scal = [M.to_host(M.gen_scalars_device(n, seed=14, stream_id=s)).reshape(n, 8) for s in range(3)]
+    ctx = M.MsmContext(d)
+    want = [ctx.msm_host(sc) for sc in scal]
+    assert (want[0] == O.msm(pts, scal[0])).all()
+    op = M.MSM(M.MsmConfig(batch_per_run=2, parts=1))
+    buf, keep = M.alloc_gpu_buffer(op.get_buffer_size(n)[0])
+    for rep in range(2):
+        res = op.run([pts], scal, [buf])
+        for i in range(3):
+            assert (res[i] == want[i]).all(), (rep, i)
+    del keep
+    # two streamed parts with the partial sum carried between them
+    op2 = M.MSM(M.MsmConfig(batch_per_run=1, parts=2))
+    buf2, keep2 = M.alloc_gpu_buffer(op2.get_buffer_size(n)[0])
+    assert (op2.run([pts], scal[:1], [buf2])[0] == want[0]).all()
+    del keep2
+    ctx.close()
+
+
+def test_reference_abi_streamed_with_tables(M):
+    # window 16 with 8 bucket sets: two window tables, both streamed
+    n = (1 << 21) + 99
+    cfg = M.MsmConfig(window_size=16, target_window=8)
+    assert cfg.get_precompute() == 2
+    d = M.gen_points_device(n, seed=15)
+    pts = M.to_host(d).reshape(n, 16)
+    tables = [pts.copy(), np.zeros_like(pts)]
+    M.MSMPrecompute(cfg).get_fn()(tables, n, 1)
+    assert (tables[1][:512] == O.precompute(pts[:512], shift=8 * 16, n_tables=2)[1]).all()
+    sc = M.to_host(M.gen_scalars_device(n, seed=15, stream_id=1)).reshape(n, 8)
+    ctx = M.MsmContext(d)
+    want = ctx.msm_host(sc)
+    op = M.MSM(cfg)
+    buf, keep = M.alloc_gpu_buffer(op.get_buffer_size(n)[0])
+    assert (op.run(tables, [sc], [buf])[0] == want).all()
+    del keep
+    # 16 parts double-buffered in two stages, two batch groups
+    cfg16 = M.MsmConfig(window_size=16, target_window=8, parts=16, batch_per_run=1, stage_scalars=2, stage_points=2)
+    op16 = M.MSM(cfg16)
+    buf16, keep16 = M.alloc_gpu_buffer(op16.get_buffer_size(n)[0])
+    sc2 = M.to_host(M.gen_scalars_device(n, seed=15, stream_id=2)).reshape(n, 8)
+    res = op16.run(tables, [sc, sc2], [buf16])
+    assert (res[0] == want).all()
+    assert (res[1] == ctx.msm_host(sc2)).all()
+    del keep16
+    ctx.close()
+
+
 def test_reference_abi_rejects_bad_arguments(M):
     op = M.MSM(M.MsmConfig(parts=0))
     with pytest.raises(M._lib.ImpellerError):

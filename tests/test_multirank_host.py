@@ -67,7 +67,10 @@ def test_msm_abi_card_split_sizes():
     assert rc == 0
     # each card plans ceil(n / 2) points: both halves smaller than the whole
     assert 0 < sizes2[0] < sizes1[0] and 0 < sizes2[1] <= sizes2[0]
-    # parts shrink the per-card buffer
-    sizes_p = (ctypes.c_ulong * 1)()
-    assert L.msm(None, sizes_p, n, 1, 4, 2, 2, 1, (ctypes.c_uint * 1)(0), None, 0, None, None) == 0
-    assert sizes_p[0] < sizes1[0]
+    # parts bound the per-card buffer for large inputs (two staged parts plus
+    # the bucket accumulators instead of the whole range)
+    big = 1 << 22
+    whole, split = (ctypes.c_ulong * 1)(), (ctypes.c_ulong * 1)()
+    assert L.msm(None, whole, big, 1, 1, 1, 1, 1, (ctypes.c_uint * 1)(0), None, 0, None, None) == 0
+    assert L.msm(None, split, big, 1, 8, 2, 2, 1, (ctypes.c_uint * 1)(0), None, 0, None, None) == 0
+    assert split[0] < whole[0] // 2
