@@ -136,9 +136,9 @@ def signed_digit_stats(scalars_canonical: np.ndarray, c: int, shared: bool = Fal
 
 # DRAM bytes per k_accumulate launch, measured with ncu (dram__bytes_read.sum
 # + dram__bytes_write.sum) on the same kernel at n = 2^21 with window tables
-# c = 20 (3.604 GB + 0.079 GB) and scaled to n = 2^22 by the number of mixed
-# additions (traffic grows in proportion): used when the run matches.
-NCU_TRAFFIC_2E22_TABLES_C20 = 7.37e9
+# c = 20 (3.607 GB + 0.071 GB) and scaled to n = 2^22 by the number of
+# entries (traffic grows in proportion): used when the run matches.
+NCU_TRAFFIC_2E22_TABLES_C20 = 7.36e9
 
 # One Fq Montgomery product is 8 rows x (8 products a_j*b_i, 1 for the
 # reduction factor, 8 products m*N_j) = 136 32x32->64-bit partial products;
@@ -259,6 +259,8 @@ def main():
     ap.add_argument("--impl", default="impeller", choices=["impeller", "reference"])
     ap.add_argument("--log2n", type=int, default=22)
     ap.add_argument("--no-extras", action="store_true", help="skip e2e / batched / CPU legs")
+    ap.add_argument("--only", default="", help="comma list of extra legs to run (e2e, resident, batched, served, cpu); "
+                                               "default all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -378,14 +380,20 @@ def main():
             "clocks": clocks,
         }
 
+    legs = set(args.only.split(",")) if args.only else {"e2e", "resident", "batched", "served", "cpu"}
     if not args.no_extras and rank == 0:
-        line["e2e"] = e2e_reference_abi(M, pts[:n], scal[0], n, c, args)
-        line["e2e_resident_srs"] = e2e_resident(M, ctx, scal[0], n, c, args)
-        line["batched"] = batched_vs_per_call(M, ctx, dev, args)
-        line["served"] = served_stream(M, ctx, dev, args)
-        pts_host = M.to_host(pts[: 1 << 20]).reshape(-1, 16)  # noqa: E501
-        sc_host = M.to_host(scal[0][: 1 << 20]).reshape(-1, 8)
-        line["cpu_baseline"] = cpu_baseline(pts_host, sc_host)
+        if "e2e" in legs:
+            line["e2e"] = e2e_reference_abi(M, pts[:n], scal[0], n, c, args)
+        if "resident" in legs:
+            line["e2e_resident_srs"] = e2e_resident(M, ctx, scal[0], n, c, args)
+        if "batched" in legs:
+            line["batched"] = batched_vs_per_call(M, ctx, dev, args)
+        if "served" in legs:
+            line["served"] = served_stream(M, ctx, dev, args)
+        if "cpu" in legs:
+            pts_host = M.to_host(pts[: 1 << 20]).reshape(-1, 16)
+            sc_host = M.to_host(scal[0][: 1 << 20]).reshape(-1, 8)
+            line["cpu_baseline"] = cpu_baseline(pts_host, sc_host)
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
