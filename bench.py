@@ -31,10 +31,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "BN254 MSM points/s at 2^22; batched vs per-call speedup; p50/p99 latency"
 UNIT = "points/s"
-# kernels of one MSM run: k_zero_words, k_histogram, k_scan_reduce,
-# k_scan_tiles, k_scan_down, k_scatter, k_accumulate, k_fixup_short,
-# k_fixup_long, k_reduce, k_window_sum, k_final
-KERNELS_PER_MSM = 12
+# kernels of one MSM run with the two-level sort: k_zero_words,
+# k_coarse_count, k_scan_reduce, k_scan_tiles, k_scan_down, k_coarse_scatter,
+# k_seg_plan, k_seg_hist, k_bin_scan, k_seg_scatter, k_accumulate,
+# k_fixup_short, k_fixup_long, k_reduce, k_window_sum, k_final
+KERNELS_PER_MSM = 16
 
 
 def env_int(name, default):

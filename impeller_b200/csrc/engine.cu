@@ -146,15 +146,39 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     p.long_cap = T;
     p.hist_grid_x = (u32)std::max<u64>(1, std::min<u64>((u64)sms * 8, (nmax + 255) / 256));
 
+    // two-level sort: tiles of scalars small enough to stage all their
+    // entries in shared memory, bins of FINE buckets, segments per bin
+    u32 wmax = 1;
+    for (const MsmDesc &d : descs) wmax = std::max(wmax, d.n_logical);
+    p.tile_scalars = std::max(32u, std::min(1024u, (STAGE_ENTRIES / wmax) & ~31u));
+    std::vector<u32> tile_first(p.M + 1);
+    u64 stiles = 0;
+    for (u32 m = 0; m < p.M; m++) {
+        tile_first[m] = (u32)stiles;
+        stiles += (descs[m].n + p.tile_scalars - 1) / p.tile_scalars;
+    }
+    tile_first[p.M] = (u32)stiles;
+    const u64 nbins = (nb + FINE - 1) / FINE;
+    p.msd = stiles > 0 && nbins <= SORT_MAX_BINS && nbins * stiles <= (1ull << 26);
+    if (p.msd) {
+        p.nbins = (u32)nbins;
+        p.sort_tiles = (u32)stiles;
+        p.cnt_pad = (u32)align_up(nbins * stiles, SCAN_TILE);
+        p.cscan_tiles = p.cnt_pad / SCAN_TILE;
+        p.segcap = (u32)((entries + SEG_ENTRIES - 1) / SEG_ENTRIES + nbins);
+    }
+
     // host image of the tables
     p.desc_off = 0;
     p.win_off = align_up(sizeof(MsmDesc) * p.M, 16);
     p.blk_off = p.win_off + align_up(sizeof(WinDesc) * wins.size(), 16);
-    const size_t tbytes = align_up(p.blk_off + sizeof(uint2) * rblocks.size(), 256);
+    p.tf_off = p.blk_off + align_up(sizeof(uint2) * rblocks.size(), 16);
+    const size_t tbytes = align_up(p.tf_off + sizeof(u32) * (p.M + 1), 256);
     p.tables.assign(tbytes, 0);
     std::memcpy(p.tables.data() + p.desc_off, descs.data(), sizeof(MsmDesc) * p.M);
     std::memcpy(p.tables.data() + p.win_off, wins.data(), sizeof(WinDesc) * wins.size());
     std::memcpy(p.tables.data() + p.blk_off, rblocks.data(), sizeof(uint2) * rblocks.size());
+    std::memcpy(p.tables.data() + p.tf_off, tile_first.data(), sizeof(u32) * (p.M + 1));
 
     // device scratch layout
     PlanLayout &lo = p.layout;
@@ -166,11 +190,23 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     };
     lo.o_tables = take(tbytes);
     lo.tables_bytes = tbytes;
-    lo.o_counts = take((size_t)p.nb_pad * 4);
-    lo.o_cursor = take((size_t)p.nb * 4);
+    lo.o_counts = take(p.msd ? 0 : (size_t)p.nb_pad * 4);
+    lo.o_cursor = take(p.msd ? 0 : (size_t)p.nb * 4);
     lo.o_offsets = take((size_t)(p.nb + 1) * 4);
-    lo.o_tiles = take((size_t)(p.ntiles + 1) * 4);
+    lo.o_tiles = take(p.msd ? 0 : (size_t)(p.ntiles + 1) * 4);
     lo.o_entries = take((size_t)std::max<u64>(entries, 1) * 4);
+    const size_t ncnt = (size_t)p.nbins * p.sort_tiles;
+    lo.o_cnt = take(p.msd ? (size_t)p.cnt_pad * 4 : 0);
+    lo.o_coff = take(p.msd ? (ncnt + 1) * 4 : 0);
+    lo.o_ccur = take(p.msd ? ncnt * 4 : 0);
+    lo.o_ctiles = take(p.msd ? (size_t)(p.cscan_tiles + 1) * 4 : 0);
+    lo.o_centry = take(p.msd ? (size_t)std::max<u64>(entries, 1) * 4 : 0);
+    lo.o_cfine = take(p.msd ? (size_t)std::max<u64>(entries, 1) * 2 : 0);
+    lo.o_segs = take(p.msd ? (size_t)p.segcap * 16 : 0);
+    lo.o_binseg = take(p.msd ? (size_t)p.nbins * 8 : 0);
+    lo.o_nsegs = take(p.msd ? 4 : 0);
+    lo.o_seghist = take(p.msd ? (size_t)p.segcap * FINE * 4 : 0);
+    lo.o_segcur = take(p.msd ? (size_t)p.segcap * FINE * 4 : 0);
     lo.o_buckets = take((size_t)p.nb * 128);
     lo.o_recb = take((size_t)2 * T * 4);
     lo.o_recp = take((size_t)2 * T * 128);
@@ -191,7 +227,7 @@ Plan::~Plan() {
         for (auto e : set) cudaEventDestroy(e);
 }
 
-u32 Plan::launches() const { return 12; }
+u32 Plan::launches() const { return msd ? 16 : 12; }
 
 const char *Plan::phase_name(int i) {
     static const char *names[NPHASE] = {"tables", "histogram", "scan", "scatter",
@@ -256,18 +292,20 @@ struct PlanPtrs {
     const MsmDesc *desc;
     const WinDesc *wins;
     const uint2 *blk;
+    const u32 *tile_first;
     u32 *counts, *cursor, *offsets, *tiles, *entries, *buckets, *recb, *recp, *parts, *parts_s, *wres, *longl;
     u32 *carry, *res;
 };
 
-static PlanPtrs plan_ptrs(const PlanLayout &L, size_t desc_off, size_t win_off, size_t blk_off, void *scratch,
-                          u32 *carry_ext, u32 *results, const void *d_image = nullptr) {
+static PlanPtrs plan_ptrs(const PlanLayout &L, size_t desc_off, size_t win_off, size_t blk_off, size_t tf_off,
+                          void *scratch, u32 *carry_ext, u32 *results, const void *d_image = nullptr) {
     unsigned char *s = static_cast<unsigned char *>(scratch);
     const unsigned char *img = d_image ? static_cast<const unsigned char *>(d_image) : s + L.o_tables;
     PlanPtrs p;
     p.desc = reinterpret_cast<const MsmDesc *>(img + desc_off);
     p.wins = reinterpret_cast<const WinDesc *>(img + win_off);
     p.blk = reinterpret_cast<const uint2 *>(img + blk_off);
+    p.tile_first = reinterpret_cast<const u32 *>(img + tf_off);
     p.counts = reinterpret_cast<u32 *>(s + L.o_counts);
     p.cursor = reinterpret_cast<u32 *>(s + L.o_cursor);
     p.offsets = reinterpret_cast<u32 *>(s + L.o_offsets);
@@ -289,6 +327,22 @@ static PlanPtrs plan_ptrs(const PlanLayout &L, size_t desc_off, size_t win_off, 
     if ((pe = prof_mark((k), st)) != cudaSuccess) \
         return pe;
 
+// k_coarse_scatter (kernel 0) and k_seg_scatter (kernel 1) stage entries in
+// up to ~200 KB of shared memory: raise their dynamic shared-memory limit
+// once per device.
+static cudaError_t sort_smem(int device, int kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, size_t> done;
+    std::lock_guard<std::mutex> g(mu);
+    size_t &have = done[std::make_pair(device, kernel)];
+    if (have >= bytes) return cudaSuccess;
+    cudaError_t e = kernel == 0
+                        ? cudaFuncSetAttribute(k_coarse_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes)
+                        : cudaFuncSetAttribute(k_seg_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) have = bytes;
+    return e;
+}
+
 // Zero n words at p and m words at q.
 __global__ void k_zero_words(u32 *__restrict__ p, u32 n, u32 *__restrict__ q, u32 m) {
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0;
@@ -302,7 +356,7 @@ __global__ void k_zero_words(u32 *__restrict__ p, u32 n, u32 *__restrict__ q, u3
 // engine.
 cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, bool record_staged,
                             const void *d_image) {
-    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, scratch, nullptr, nullptr, d_image);
+    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, tf_off, scratch, nullptr, nullptr, d_image);
     cudaError_t pe;
     MARK(0);
     if (!d_image) {
@@ -310,26 +364,70 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
                            cudaMemcpyHostToDevice, st));
         if (record_staged) CK(cudaEventRecord(staged, st));
     }
-    // the bucket counts and the long-run counter of the fixups
-    k_zero_words<<<std::max(1u, std::min((nb_pad + 255) / 256, (u32)sm_count(device) * 4)), 256, 0, st>>>(
-        p.counts, nb_pad, p.longl, 1);
-    CK_LAUNCH("k_zero_words");
-    MARK(1);
+    if (msd) {
+        unsigned char *sb = static_cast<unsigned char *>(scratch);
+        u32 *cnt = reinterpret_cast<u32 *>(sb + layout.o_cnt);
+        u32 *coff = reinterpret_cast<u32 *>(sb + layout.o_coff);
+        u32 *ccur = reinterpret_cast<u32 *>(sb + layout.o_ccur);
+        u32 *ctiles = reinterpret_cast<u32 *>(sb + layout.o_ctiles);
+        const u32 ncnt = nbins * sort_tiles;
+        SortArgs sa{p.desc, p.tile_first, M, sort_tiles, tile_scalars, nbins, nb, segcap, cnt, coff,
+                    reinterpret_cast<u32 *>(sb + layout.o_centry),
+                    reinterpret_cast<unsigned short *>(sb + layout.o_cfine),
+                    reinterpret_cast<uint4 *>(sb + layout.o_segs), reinterpret_cast<uint2 *>(sb + layout.o_binseg),
+                    reinterpret_cast<u32 *>(sb + layout.o_nsegs), reinterpret_cast<u32 *>(sb + layout.o_seghist),
+                    reinterpret_cast<u32 *>(sb + layout.o_segcur), p.offsets, p.entries};
+        // the scan padding of the tile counts and the long-run counter of the fixups
+        k_zero_words<<<1, 256, 0, st>>>(cnt + ncnt, cnt_pad - ncnt, p.longl, 1);
+        CK_LAUNCH("k_zero_words");
+        MARK(1);
+        k_coarse_count<<<sort_tiles, SORT_BLOCK, nbins * 4, st>>>(sa);
+        CK_LAUNCH("k_coarse_count");
+        MARK(2);
+        k_scan_reduce<<<cscan_tiles, SCAN_BLOCK, 0, st>>>(cnt, ctiles);
+        CK_LAUNCH("k_scan_reduce");
+        k_scan_tiles<<<1, SCAN_BLOCK, 0, st>>>(ctiles, cscan_tiles);
+        CK_LAUNCH("k_scan_tiles");
+        k_scan_down<<<cscan_tiles, SCAN_BLOCK, 0, st>>>(cnt, ctiles, coff, ccur, ncnt, cscan_tiles);
+        CK_LAUNCH("k_scan_down");
+        MARK(3);
+        const size_t scatter_smem = ((size_t)2 * nbins + 2 * STAGE_ENTRIES) * 4;
+        CK(sort_smem(device, 0, scatter_smem));
+        k_coarse_scatter<<<sort_tiles, SORT_BLOCK, scatter_smem, st>>>(sa);
+        CK_LAUNCH("k_coarse_scatter");
+        k_seg_plan<<<1, FINE_BLOCK, 0, st>>>(sa);
+        CK_LAUNCH("k_seg_plan");
+        k_seg_hist<<<segcap, FINE_BLOCK, 0, st>>>(sa);
+        CK_LAUNCH("k_seg_hist");
+        k_bin_scan<<<nbins, FINE_BLOCK, 0, st>>>(sa);
+        CK_LAUNCH("k_bin_scan");
+        const size_t seg_smem = (size_t)2 * FINE * 4 + (size_t)SEG_ENTRIES * 6;
+        CK(sort_smem(device, 1, seg_smem));
+        k_seg_scatter<<<segcap, FINE_BLOCK, seg_smem, st>>>(sa);
+        CK_LAUNCH("k_seg_scatter");
+        MARK(4);
+    } else {
+        // the bucket counts and the long-run counter of the fixups
+        k_zero_words<<<std::max(1u, std::min((nb_pad + 255) / 256, (u32)sm_count(device) * 4)), 256, 0, st>>>(
+            p.counts, nb_pad, p.longl, 1);
+        CK_LAUNCH("k_zero_words");
+        MARK(1);
 
-    dim3 hgrid(hist_grid_x, M);
-    k_histogram<<<hgrid, 256, 0, st>>>(p.desc, p.counts);
-    CK_LAUNCH("k_histogram");
-    MARK(2);
-    k_scan_reduce<<<ntiles, SCAN_BLOCK, 0, st>>>(p.counts, p.tiles);
-    CK_LAUNCH("k_scan_reduce");
-    k_scan_tiles<<<1, SCAN_BLOCK, 0, st>>>(p.tiles, ntiles);
-    CK_LAUNCH("k_scan_tiles");
-    k_scan_down<<<ntiles, SCAN_BLOCK, 0, st>>>(p.counts, p.tiles, p.offsets, p.cursor, nb, ntiles);
-    CK_LAUNCH("k_scan_down");
-    MARK(3);
-    k_scatter<<<hgrid, 256, 0, st>>>(p.desc, p.cursor, p.entries);
-    CK_LAUNCH("k_scatter");
-    MARK(4);
+        dim3 hgrid(hist_grid_x, M);
+        k_histogram<<<hgrid, 256, 0, st>>>(p.desc, p.counts);
+        CK_LAUNCH("k_histogram");
+        MARK(2);
+        k_scan_reduce<<<ntiles, SCAN_BLOCK, 0, st>>>(p.counts, p.tiles);
+        CK_LAUNCH("k_scan_reduce");
+        k_scan_tiles<<<1, SCAN_BLOCK, 0, st>>>(p.tiles, ntiles);
+        CK_LAUNCH("k_scan_tiles");
+        k_scan_down<<<ntiles, SCAN_BLOCK, 0, st>>>(p.counts, p.tiles, p.offsets, p.cursor, nb, ntiles);
+        CK_LAUNCH("k_scan_down");
+        MARK(3);
+        k_scatter<<<hgrid, 256, 0, st>>>(p.desc, p.cursor, p.entries);
+        CK_LAUNCH("k_scatter");
+        MARK(4);
+    }
 
     AccumArgs aa{p.entries, p.offsets, nb, points, p.buckets, p.recb, p.recp};
     k_accumulate<<<accum_blocks, accum_block, 0, st>>>(aa);
@@ -350,7 +448,7 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
 // `buckets` (the plan's own, sparse by offsets, or dense accumulators).
 cudaError_t Plan::run_tail(void *scratch, const u32 *buckets, bool dense, u32 *results, int carry_mode,
                            cudaStream_t st, u32 *carry_ext, const void *d_image) {
-    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, scratch, carry_ext, results, d_image);
+    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, tf_off, scratch, carry_ext, results, d_image);
     cudaError_t pe;
     ReduceArgs ra{p.wins, p.blk, p.offsets, buckets, p.parts, p.parts_s, dense ? 1u : 0u};
     k_reduce<<<nrblocks, REDUCE_BLOCK, 0, st>>>(ra);
@@ -388,7 +486,7 @@ cudaError_t Plan::launch_chunk(void *scratch, const u32 *points, u32 *acc, bool 
                                const void *d_image) {
     cudaError_t e = run_front(scratch, points, st, true, d_image);
     if (e != cudaSuccess) return e;
-    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, scratch, nullptr, nullptr, d_image);
+    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, tf_off, scratch, nullptr, nullptr, d_image);
     const u32 blocks = std::max(1u, std::min((nb + 255) / 256, (u32)sm_count(device) * 8));
     k_bucket_merge<<<blocks, 256, 0, st>>>(p.offsets, p.buckets, acc, nb, first ? 1u : 0u);
     CK_LAUNCH("k_bucket_merge");

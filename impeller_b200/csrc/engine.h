@@ -37,9 +37,11 @@ u32 table_window(u64 n);    // tables window the autotune table recommends (0: n
 int sm_count(int device);
 
 struct PlanLayout {
-    size_t o_tables, tables_bytes;  // descs | wins | reduce blocks (uploaded each run)
+    size_t o_tables, tables_bytes;  // descs | wins | reduce blocks | sort tiles (uploaded each run)
     size_t o_counts, o_cursor, o_offsets, o_tiles, o_entries, o_buckets;
     size_t o_recb, o_recp, o_parts, o_parts_s, o_wres, o_long, o_carry, o_results;
+    // two-level sort
+    size_t o_cnt, o_coff, o_ccur, o_ctiles, o_centry, o_cfine, o_segs, o_binseg, o_nsegs, o_seghist, o_segcur;
     size_t bytes;
 };
 
@@ -106,6 +108,9 @@ class Plan {
     u32 accum_blocks = 0, accum_block = 256;
     u32 nparts = 0, long_cap = 0;
     u32 hist_grid_x = 1;
+    // two-level sort (msd) or per-entry atomic bucket sort
+    bool msd = false;
+    u32 nbins = 0, sort_tiles = 0, tile_scalars = 0, segcap = 0, cnt_pad = 0, cscan_tiles = 0;
     std::vector<MsmShape> shapes;
     PlanLayout layout{};
 
@@ -131,7 +136,7 @@ class Plan {
     size_t ext_cap = 0;
     cudaEvent_t staged = nullptr;
     std::vector<unsigned char> tables;  // host image of the tables
-    size_t desc_off = 0, win_off = 0, blk_off = 0;
+    size_t desc_off = 0, win_off = 0, blk_off = 0, tf_off = 0;
     u32 nwins = 0, nrblocks = 0;
     bool profiling = false;
     std::vector<std::vector<cudaEvent_t>> prof_sets;  // one set of NPHASE+1 events per run

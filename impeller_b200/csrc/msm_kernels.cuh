@@ -66,25 +66,20 @@ struct WinDesc {
     u32 pad0, pad1;
 };
 
-__device__ __forceinline__ u32 limb_at(const Fr &v, u32 idx) {
-    u32 r = 0;
-#pragma unroll
-    for (u32 k = 0; k < 8; k++)
-        if (k == idx) r = v.l[k];
-    return r;
-}
-
 // Signed-digit recoding of the reference (core/src/msm/src/msm_impl.cuh:22-33):
 // a digit >= 2^(c-1) becomes digit - 2^c and carries into the next window.
 // The top window is never recoded: for every 3 <= c <= 31, r < 2^254 keeps
 // the top digit plus an incoming carry at most 2^(c-1), a valid bucket.
+// Windows are taken in order, w = 0, 1, ...: the scalar is shifted right by
+// c after each window, so the next digit is always the low c bits of limb 0.
 struct DigitIter {
     Fr v;
     u32 c, carry;
     __device__ __forceinline__ void next(u32 w, u32 n_logical, u32 &mag, u32 &sign) {
-        u32 o = w * c;
-        u32 idx = o >> 5, sh = o & 31u;
-        u32 raw = __funnelshift_r(limb_at(v, idx), limb_at(v, idx + 1), sh) & ((1u << c) - 1u);
+        const u32 raw = v.l[0] & ((1u << c) - 1u);
+#pragma unroll
+        for (int k = 0; k < 7; k++) v.l[k] = __funnelshift_r(v.l[k], v.l[k + 1], c);
+        v.l[7] >>= c;
         u32 d = raw + carry;
         u32 half = 1u << (c - 1);
         if (d >= half && w + 1 < n_logical) {
@@ -155,6 +150,277 @@ __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ c
             }
         }
     }
+}
+
+// ------------------------------------------------- two-level counting sort
+//
+// The bucket sort above costs one L2 atomic per entry in each of its two
+// passes and scatters 4-byte writes over the whole entry array.  The
+// two-level sort keeps every atomic in shared memory and every global write
+// in runs:
+//   k_coarse_count    per tile of scalars: entries per coarse bin (the top
+//                     bits of the global bucket index; FINE buckets per bin)
+//   (scan)            bin-major exclusive scan of the tile counts
+//   k_coarse_scatter  per tile: entries staged in shared memory in bin order,
+//                     written out as one contiguous run per bin, with the
+//                     fine index (bucket within the bin) beside them
+//   k_seg_plan        split every bin into segments of at most SEG_ENTRIES
+//   k_seg_hist        per segment: entries per fine bucket
+//   k_bin_scan        per bin: bucket offsets, and each segment's cursor per
+//                     fine bucket
+//   k_seg_scatter     per segment: entries staged in bucket order, written
+//                     to their final slots as one run per bucket
+// Order inside a bucket is irrelevant (a bucket is a sum).  Heavy buckets
+// (skewed scalars) only lengthen their bin, which splits into more segments.
+// Shared-memory atomics are taken per lane: a per-lane atomicAdd on a cursor
+// already returns a distinct slot, and warp matching to aggregate them
+// measured slower than the atomics it saves.
+
+static constexpr u32 FINE_BITS = 10;
+static constexpr u32 FINE = 1u << FINE_BITS;     // buckets per coarse bin
+static constexpr u32 SORT_MAX_BINS = 8192;       // nb <= 2^23
+static constexpr u32 STAGE_ENTRIES = 16384;      // staged entries per tile
+static constexpr u32 SEG_ENTRIES = 32768;        // entries per fine segment (staged whole)
+static constexpr u32 SORT_BLOCK = 512;
+static constexpr u32 FINE_BLOCK = 1024;
+static_assert(FINE == FINE_BLOCK, "k_seg_scatter gives every bucket of a bin one thread");
+
+struct SortArgs {
+    const MsmDesc *descs;
+    const u32 *tile_first;  // M + 1: first sort tile of each MSM
+    u32 M, ntiles, tile_scalars, nbins, nb, segcap;
+    u32 *cnt;               // nbins x ntiles, bin-major (scan input, padded)
+    const u32 *coff;        // exclusive scan of cnt; coff[nbins * ntiles] = E
+    u32 *c_entry;           // entries in coarse order
+    unsigned short *c_fine; // their bucket index within the bin
+    uint4 *segs;            // per segment: bin, first, end
+    uint2 *bin_seg;         // per bin: first segment, segment count
+    u32 *nsegs;             // [0]: number of segments
+    u32 *seghist;           // segcap x FINE: entries per segment and bucket
+    u32 *segcur;            // segcap x FINE: each segment's first slot per bucket
+    u32 *offsets;           // nb + 1 (output)
+    u32 *entries;           // (output)
+};
+
+// Exclusive scan over the block (blockDim a multiple of 32, at most 1024).
+__device__ __forceinline__ u32 block_scan_excl(u32 v, u32 &total, u32 *warp_tot) {
+    const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    u32 x = v;
+#pragma unroll
+    for (u32 o = 1; o < 32; o <<= 1) {
+        u32 y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        u32 t = lane < nw ? warp_tot[lane] : 0;
+#pragma unroll
+        for (u32 o = 1; o < 32; o <<= 1) {
+            u32 y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < nw) warp_tot[lane] = t;
+    }
+    __syncthreads();
+    total = warp_tot[nw - 1];
+    const u32 before = wid ? warp_tot[wid - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+// MSM and scalar range [start, end) of a sort tile (tiles of one MSM are
+// consecutive; the largest m with tile_first[m] <= tile owns it).
+__device__ __forceinline__ void sort_tile(const SortArgs &a, u32 tile, u32 &m, u32 &start, u32 &end) {
+    u32 lo = 0, hi = a.M;
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (a.tile_first[mid] <= tile) lo = mid;
+        else hi = mid;
+    }
+    m = lo;
+    start = (tile - a.tile_first[m]) * a.tile_scalars;
+    end = min(start + a.tile_scalars, a.descs[m].n);
+}
+
+__global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
+    extern __shared__ u32 hist[];  // nbins
+    u32 m, start, end;
+    sort_tile(a, blockIdx.x, m, start, end);
+    const MsmDesc d = a.descs[m];
+    for (u32 b = threadIdx.x; b < a.nbins; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    const u32 B = 1u << (d.c - 1);
+    for (u32 base = start; base < end; base += blockDim.x) {
+        const u32 i = base + threadIdx.x;
+        const bool live = i < end;
+        DigitIter it;
+        it.v = live ? fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i)) : fe_zero<FrP>();
+        it.c = d.c;
+        it.carry = 0;
+        for (u32 w = 0; w < d.n_logical; w++) {
+            u32 mag, sign;
+            it.next(w, d.n_logical, mag, sign);
+            if (mag) atomicAdd(&hist[(d.bucket_base + (w % d.n_windows) * B + mag - 1) >> FINE_BITS], 1u);
+        }
+    }
+    __syncthreads();
+    for (u32 b = threadIdx.x; b < a.nbins; b += blockDim.x) a.cnt[(size_t)b * a.ntiles + blockIdx.x] = hist[b];
+}
+
+// Shared memory: delta[nbins], cur[nbins], stage_e[STAGE_ENTRIES],
+// stage_f[STAGE_ENTRIES].  A tile holds at most STAGE_ENTRIES entries (the
+// plan sizes tiles by the largest window count).
+__global__ void __launch_bounds__(SORT_BLOCK) k_coarse_scatter(SortArgs a) {
+    extern __shared__ u32 sm[];
+    __shared__ u32 warp_tot[32];
+    u32 *delta = sm, *cur = sm + a.nbins, *stage_e = sm + 2 * a.nbins, *stage_f = stage_e + STAGE_ENTRIES;
+    const u32 tile = blockIdx.x;
+    u32 m, start, end;
+    sort_tile(a, tile, m, start, end);
+    const MsmDesc d = a.descs[m];
+    // this tile's bins: local start (exclusive scan of its counts) and the
+    // distance from a local slot to the global coarse position
+    const u32 per = (a.nbins + blockDim.x - 1) / blockDim.x;
+    const u32 b0 = threadIdx.x * per;
+    u32 sum = 0;
+    for (u32 k = 0; k < per; k++)
+        if (b0 + k < a.nbins) sum += a.cnt[(size_t)(b0 + k) * a.ntiles + tile];
+    u32 total;
+    u32 run = block_scan_excl(sum, total, warp_tot);
+    for (u32 k = 0; k < per; k++) {
+        const u32 b = b0 + k;
+        if (b < a.nbins) {
+            const size_t ci = (size_t)b * a.ntiles + tile;
+            cur[b] = run;
+            delta[b] = a.coff[ci] - run;
+            run += a.cnt[ci];
+        }
+    }
+    __syncthreads();
+    const u32 B = 1u << (d.c - 1);
+    for (u32 base = start; base < end; base += blockDim.x) {
+        const u32 i = base + threadIdx.x;
+        const bool live = i < end;
+        DigitIter it;
+        it.v = live ? fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i)) : fe_zero<FrP>();
+        it.c = d.c;
+        it.carry = 0;
+        for (u32 w = 0; w < d.n_logical; w++) {
+            u32 mag, sign;
+            it.next(w, d.n_logical, mag, sign);
+            if (mag) {
+                const u32 key = d.bucket_base + (w % d.n_windows) * B + mag - 1;
+                const u32 bin = key >> FINE_BITS;
+                const u32 slot = atomicAdd(&cur[bin], 1u);
+                const u32 table = w / d.n_windows;
+                stage_e[slot] = ((d.table_base + table * d.table_stride + i) << 1) | sign;
+                stage_f[slot] = (key & (FINE - 1u)) | (bin << 16);
+            }
+        }
+    }
+    __syncthreads();
+    for (u32 s = threadIdx.x; s < total; s += blockDim.x) {
+        const u32 f = stage_f[s];
+        const u32 pos = delta[f >> 16] + s;
+        a.c_entry[pos] = stage_e[s];
+        a.c_fine[pos] = (unsigned short)(f & 0xffffu);
+    }
+}
+
+// One block: every bin's segments (at most SEG_ENTRIES entries each).
+__global__ void __launch_bounds__(FINE_BLOCK) k_seg_plan(SortArgs a) {
+    __shared__ u32 warp_tot[32];
+    const u32 per = (a.nbins + blockDim.x - 1) / blockDim.x;
+    const u32 b0 = threadIdx.x * per;
+    u32 sum = 0;
+    for (u32 k = 0; k < per; k++) {
+        const u32 b = b0 + k;
+        if (b < a.nbins) {
+            const u32 size = a.coff[(size_t)(b + 1) * a.ntiles] - a.coff[(size_t)b * a.ntiles];
+            sum += (size + SEG_ENTRIES - 1) / SEG_ENTRIES;
+        }
+    }
+    u32 total;
+    u32 run = block_scan_excl(sum, total, warp_tot);
+    for (u32 k = 0; k < per; k++) {
+        const u32 b = b0 + k;
+        if (b < a.nbins) {
+            const u32 bs = a.coff[(size_t)b * a.ntiles], be = a.coff[(size_t)(b + 1) * a.ntiles];
+            const u32 ns = (be - bs + SEG_ENTRIES - 1) / SEG_ENTRIES;
+            a.bin_seg[b] = make_uint2(run, ns);
+            for (u32 j = 0; j < ns; j++)
+                a.segs[run + j] = make_uint4(b, bs + j * SEG_ENTRIES, min(bs + (j + 1) * SEG_ENTRIES, be), 0u);
+            run += ns;
+        }
+    }
+    if (threadIdx.x == 0) a.nsegs[0] = total;
+}
+
+__global__ void __launch_bounds__(FINE_BLOCK) k_seg_hist(SortArgs a) {
+    __shared__ u32 hist[FINE];
+    if (blockIdx.x >= a.nsegs[0]) return;
+    const uint4 sg = a.segs[blockIdx.x];
+    for (u32 f = threadIdx.x; f < FINE; f += blockDim.x) hist[f] = 0;
+    __syncthreads();
+    for (u32 i = sg.y + threadIdx.x; i < sg.z; i += blockDim.x) atomicAdd(&hist[a.c_fine[i]], 1u);
+    __syncthreads();
+    for (u32 f = threadIdx.x; f < FINE; f += blockDim.x) a.seghist[(size_t)blockIdx.x * FINE + f] = hist[f];
+}
+
+// One block per bin: per fine bucket, an exclusive scan over the bin's
+// segments (their cursors) and the bucket's total; then a scan over the
+// bin's buckets gives the bucket offsets.
+__global__ void __launch_bounds__(FINE_BLOCK) k_bin_scan(SortArgs a) {
+    __shared__ u32 warp_tot[32];
+    const u32 b = blockIdx.x;
+    const uint2 bs = a.bin_seg[b];
+    const u32 base = a.coff[(size_t)b * a.ntiles];
+    u32 carry = base;
+    for (u32 f0 = 0; f0 < FINE; f0 += blockDim.x) {
+        const u32 f = f0 + threadIdx.x;
+        u32 run = 0;
+        for (u32 s = bs.x; s < bs.x + bs.y; s++) run += a.seghist[(size_t)s * FINE + f];
+        u32 total;
+        const u32 off = carry + block_scan_excl(run, total, warp_tot);
+        const u32 g = b * FINE + f;
+        if (g < a.nb) a.offsets[g] = off;
+        // each segment's cursor: the bucket offset plus the earlier segments' counts
+        u32 cur = off;
+        for (u32 s = bs.x; s < bs.x + bs.y; s++) {
+            a.segcur[(size_t)s * FINE + f] = cur;
+            cur += a.seghist[(size_t)s * FINE + f];
+        }
+        carry += total;
+    }
+    if (b == a.nbins - 1 && threadIdx.x == 0) a.offsets[a.nb] = a.coff[(size_t)a.nbins * a.ntiles];
+}
+
+// Shared memory: lcur[FINE], delta[FINE], stage_e[SEG_ENTRIES],
+// stage_f[SEG_ENTRIES] (16-bit).
+__global__ void __launch_bounds__(FINE_BLOCK) k_seg_scatter(SortArgs a) {
+    extern __shared__ u32 sm[];
+    __shared__ u32 warp_tot[32];
+    if (blockIdx.x >= a.nsegs[0]) return;
+    u32 *lcur = sm, *delta = sm + FINE, *stage_e = sm + 2 * FINE;
+    unsigned short *stage_f = reinterpret_cast<unsigned short *>(stage_e + SEG_ENTRIES);
+    const uint4 sg = a.segs[blockIdx.x];
+    const size_t h = (size_t)blockIdx.x * FINE;
+    // local exclusive scan of this segment's counts (FINE == blockDim.x)
+    const u32 f = threadIdx.x;
+    u32 total;
+    const u32 ls = block_scan_excl(a.seghist[h + f], total, warp_tot);
+    lcur[f] = ls;
+    delta[f] = a.segcur[h + f] - ls;
+    __syncthreads();
+    for (u32 i = sg.y + threadIdx.x; i < sg.z; i += blockDim.x) {
+        const u32 fi = a.c_fine[i];
+        const u32 slot = atomicAdd(&lcur[fi], 1u);
+        stage_e[slot] = a.c_entry[i];
+        stage_f[slot] = (unsigned short)fi;
+    }
+    __syncthreads();
+    for (u32 s = threadIdx.x; s < total; s += blockDim.x) a.entries[delta[stage_f[s]] + s] = stage_e[s];
 }
 
 // ------------------------------------------------------------------- scan
