@@ -29,9 +29,13 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE_PATH = os.path.join(HERE, "autotune_table.json")
 
-# window tables for these c only: their top digit window keeps >= 12 bits,
-# so the shared bucket set is not flooded by the short top window
+# window tables: c >= 16 for n >= 2^14, where their top digit window keeps
+# >= 12 bits so the shared bucket set is not flooded by the short top window;
+# small c for small n, where the flooding is bounded by n and a single shared
+# bucket set saves the plain path's Horner tail (about 250 doublings).
 TABLE_WINDOWS = (16, 18, 20, 22)
+SMALL_TABLE_WINDOWS = (8, 10, 12, 13)
+SMALL_TABLE_MAX_LOG2N = 17
 
 
 def plain_candidates(k: int) -> list:
@@ -71,9 +75,11 @@ def tune(kmin: int = 10, kmax: int = 23, reps: int = 5, device: int = 0, out: st
         entries[k].update(plain_c=best[1], plain_ms=round(best[0], 4))
         print(json.dumps(entries[k]), flush=True)
     tab = {k: (math.inf, 0) for k in entries}
-    for ct in TABLE_WINDOWS:
+    for ct in SMALL_TABLE_WINDOWS + TABLE_WINDOWS:
         ctx.precompute(ct)
-        for k in range(max(kmin, 14), kmax + 1):
+        ks = range(kmin, min(kmax, SMALL_TABLE_MAX_LOG2N) + 1) if ct in SMALL_TABLE_WINDOWS \
+            else range(max(kmin, 14), kmax + 1)
+        for k in ks:
             n = 1 << k
             t = _time(ctx, scal, n, ct, max(2, reps // 2))
             if t < tab[k][0]:
