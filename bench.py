@@ -260,8 +260,8 @@ def main():
     ap.add_argument("--impl", default="impeller", choices=["impeller", "reference"])
     ap.add_argument("--log2n", type=int, default=22)
     ap.add_argument("--no-extras", action="store_true", help="skip e2e / batched / CPU legs")
-    ap.add_argument("--only", default="", help="comma list of extra legs to run (e2e, resident, batched, served, cpu); "
-                                               "default all")
+    ap.add_argument("--only", default="", help="comma list of extra legs to run (e2e, resident, batched, served, cpu, "
+                                               "bls12381); default all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -381,7 +381,7 @@ def main():
             "clocks": clocks,
         }
 
-    legs = set(args.only.split(",")) if args.only else {"e2e", "resident", "batched", "served", "cpu"}
+    legs = set(args.only.split(",")) if args.only else {"e2e", "resident", "batched", "served", "cpu", "bls12381"}
     if not args.no_extras and rank == 0:
         if "e2e" in legs:
             line["e2e"] = e2e_reference_abi(M, pts[:n], scal[0], n, c, args)
@@ -395,6 +395,12 @@ def main():
             pts_host = M.to_host(pts[: 1 << 20]).reshape(-1, 16)
             sc_host = M.to_host(scal[0][: 1 << 20]).reshape(-1, 8)
             line["cpu_baseline"] = cpu_baseline(pts_host, sc_host)
+    if not args.no_extras and rank == 0 and "bls12381" in legs:
+        del scal
+        ctx.close()
+        del pts
+        torch.cuda.empty_cache()
+        line["bls12381"] = bls12381_leg(M, dev, n, args)
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -428,6 +434,62 @@ def e2e_reference_abi(M, d_pts, d_scal, n, c, args) -> dict:
     del keep
     return {"value": n / dt, "unit": UNIT, "h2d_bytes_per_step": n * (64 + 32), "d2h_bytes_per_step": 64,
             "ms_per_step": dt * 1e3, "api": f"msm() C ABI ({M.lib_name(cfg)}), pinned host buffers, wall clock"}
+
+
+def bls12381_leg(M, dev, n, args) -> dict:
+    """The same MSM on the reference's second curve, BLS12-381 G1 (381-bit
+    base field in 12 limbs, 255-bit scalars): device-resident inputs timed
+    with CUDA events (resident window tables where the autotune table puts
+    them), then the drop-in msm() C ABI of lib/libmsm_bls12381_{c}_{alpha}
+    on pinned host buffers, wall clock."""
+    import torch
+    C = M.BLS12381
+    pts = M.gen_points_device(n, seed=0, device=dev, curve=C)
+    scal = [M.gen_scalars_device(n, seed=0, stream_id=1 + v, device=dev, curve=C) for v in range(4)]
+    ctx = M.MsmContext(pts, device=dev, curve=C)
+    c_tab = M.table_window(n)
+    if c_tab:
+        ctx.precompute(c_tab)
+    c = ctx.window(n)
+    outs = [torch.empty(24, dtype=torch.int32, device=f"cuda:{dev}") for _ in range(4)]
+    stream = torch.cuda.current_stream()
+    for w in range(args.warmup):
+        ctx.msm_device(scal[w % 4], c=c, out=outs[w % 4])
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        ctx.msm_device(scal[k % 4], c=c, out=outs[k % 4])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    ctx.close()
+    # drop-in ABI, host buffers
+    cd = M.default_window(n)
+    cfg = M.MsmConfig(window_size=cd, target_window=M.window_count(cd, C), curve=C)
+    op = M.MSM(cfg)
+    buf, keep = M.alloc_gpu_buffer(op.get_buffer_size(n)[0], device=dev)
+    hp = torch.empty((n, 24), dtype=torch.int32, pin_memory=True)
+    hs = torch.empty((n, 8), dtype=torch.int32, pin_memory=True)
+    hp.copy_(pts.cpu())
+    hs.copy_(scal[0].cpu())
+    del pts, scal
+    pts_np, sc_np = hp.numpy().view(np.uint32), hs.numpy().view(np.uint32)
+    for _ in range(2):
+        op.run([pts_np], [sc_np], [buf])
+    steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        op.run([pts_np], [sc_np], [buf])
+    dt = (time.perf_counter() - t0) / steps
+    del keep
+    return {"workload": f"single BLS12-381 G1 MSM, n=2^{int(math.log2(n))}, window c={c}",
+            "window_tables": bool(c_tab), "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "timing": "CUDA events, inputs resident, 4 rotating scalar vectors (> L2)",
+            "e2e": {"value": n / dt, "unit": UNIT, "h2d_bytes_per_step": n * (96 + 32), "d2h_bytes_per_step": 96,
+                    "ms_per_step": dt * 1e3, "api": f"msm() C ABI ({M.lib_name(cfg)}), pinned host buffers, "
+                                                    "wall clock"}}
 
 
 def e2e_resident(M, ctx, d_scal, n, c, args) -> dict:

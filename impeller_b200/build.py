@@ -98,12 +98,15 @@ def build(verbose: bool = False, ptxas_v: bool = False, force: bool = False) -> 
 SHIM_DIR = os.path.join(HERE, "lib")
 
 
-def build_shim(window_size: int, target_window: int, debug: bool = False) -> str:
-    """lib/libmsm_bn254_{c}_{alpha}_{debug}.so forwarding to libimpeller_msm.so
+CURVE_NAMES = ("bn254", "bls12381")
+
+
+def build_shim(window_size: int, target_window: int, debug: bool = False, curve: int = 0) -> str:
+    """lib/libmsm_{curve}_{c}_{alpha}_{debug}.so forwarding to libimpeller_msm.so
     (rpath $ORIGIN/..), the reference's per-configuration library name."""
     core = build()
     os.makedirs(SHIM_DIR, exist_ok=True)
-    name = f"libmsm_bn254_{window_size}_{target_window}_{'true' if debug else 'false'}.so"
+    name = f"libmsm_{CURVE_NAMES[curve]}_{window_size}_{target_window}_{'true' if debug else 'false'}.so"
     out = os.path.join(SHIM_DIR, name)
     src = os.path.join(CSRC, "shim", "msm_shim.c")
     if not _stale(out, [src, core, os.path.join(ROOT, "include", "impeller_msm.h")]):
@@ -111,6 +114,7 @@ def build_shim(window_size: int, target_window: int, debug: bool = False) -> str
     cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc())), "include")
     cmd = ["gcc", "-O2", "-shared", "-fPIC", f"-DMSM_WINDOW_SIZE={int(window_size)}",
            f"-DMSM_TARGET_WINDOWS={int(target_window)}", f"-DMSM_DEBUG={1 if debug else 0}",
+           f"-DMSM_CURVE_ID={int(curve)}",
            "-I" + os.path.join(ROOT, "include"), "-I" + cuda_inc, src, "-o", out + ".tmp",
            "-L" + HERE, "-limpeller_msm", "-Wl,-rpath,$ORIGIN/.."]
     r = subprocess.run(cmd, capture_output=True, text=True)

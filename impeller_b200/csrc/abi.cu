@@ -56,9 +56,15 @@ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 struct Config {
     u32 c, W, n_windows, n_tables;
     bool debug;
+    u32 curve;
+    u32 PW, XW;  // affine and XYZZ point words
 };
 
-bool make_config(unsigned window_size, unsigned target_window, int debug, Config &cfg) {
+bool make_config(unsigned window_size, unsigned target_window, int debug, Config &cfg, u32 curve = CURVE_BN254) {
+    if (curve != CURVE_BN254 && curve != CURVE_BLS12381) {
+        set_error("unknown curve");
+        return false;
+    }
     if (window_size < 3 || window_size > 31) {
         set_error("window_size must be in [3, 31]");
         return false;
@@ -68,10 +74,27 @@ bool make_config(unsigned window_size, unsigned target_window, int debug, Config
         return false;
     }
     cfg.c = window_size;
-    cfg.W = digit_windows(window_size);
+    cfg.curve = curve;
+    cfg.PW = point_words(curve);
+    cfg.XW = xyzz_words(curve);
+    cfg.W = digit_windows(window_size, curve);
     cfg.n_windows = std::min(cfg.W, target_window);
     cfg.n_tables = (cfg.W + cfg.n_windows - 1) / cfg.n_windows;
     cfg.debug = debug != 0;
+    // The caller allocates the reference's number of window tables,
+    // ceil(ceil(bits / c) / n_windows) (common/src/msm_config.rs:17-25).
+    // BLS12-381 scalars need one more signed-digit window than ceil(255 / c)
+    // for c = 3, 5, 15, 17; refuse a configuration whose table count would
+    // then differ from the caller's.
+    const u32 bits = curve == CURVE_BLS12381 ? 255u : 254u;
+    const u32 ref_w = (bits + window_size - 1) / window_size;
+    const u32 ref_nw = std::min(ref_w, target_window);
+    if ((ref_w + ref_nw - 1) / ref_nw != cfg.n_tables) {
+        set_error("window size " + std::to_string(window_size) + " with target window " +
+                  std::to_string(target_window) +
+                  " needs one more signed-digit window than the reference's table layout on this curve");
+        return false;
+    }
     return true;
 }
 
@@ -93,7 +116,7 @@ u32 stream_chunks(u64 len) {
 constexpr u32 PART_STAGES = 2;
 
 std::vector<MsmShape> group_shapes(const Config &cfg, u32 M, u32 n, u32 part_len) {
-    std::vector<MsmShape> s(M, MsmShape{n, cfg.c, cfg.n_windows, part_len, 0});
+    std::vector<MsmShape> s(M, MsmShape{n, cfg.c, cfg.n_windows, part_len, 0, cfg.curve});
     return s;
 }
 
@@ -127,11 +150,11 @@ bool card_layout(const Config &cfg, int device, u64 len, u32 num_cards, u32 card
         off = align_up(off + b, 256);
         return o;
     };
-    L.o_points = take(stages * cfg.n_tables * L.part_len * 64);
+    L.o_points = take(stages * cfg.n_tables * L.part_len * cfg.PW * 4);
     L.o_scalars = take(stages * batch_per_run * L.part_len * 32);
-    L.o_carry = take((size_t)batch_per_run * 128);
-    L.o_results = take((size_t)batch_per_run * 64);
-    L.o_combine = take((size_t)num_cards * 128 + 64);
+    L.o_carry = take((size_t)batch_per_run * cfg.XW * 4);
+    L.o_results = take((size_t)batch_per_run * cfg.PW * 4);
+    L.o_combine = take((size_t)num_cards * cfg.XW * 4 + cfg.PW * 4);
     L.o_plan = take(plan_bytes);
     L.o_acc = take(acc_bytes);
     L.o_images = take(images);
@@ -204,7 +227,7 @@ DevicePlans &device_plans(int device) {
 constexpr size_t PLAN_CACHE_CAP = 32;
 
 Plan *cached_plan(DevicePlans &D, int device, const Config &cfg, u32 M, u32 n, u32 stride) {
-    std::vector<u32> key{cfg.c, cfg.n_windows, M, n, stride};
+    std::vector<u32> key{cfg.c, cfg.n_windows, M, n, stride, cfg.curve};
     auto it = D.plans.find(key);
     if (it != D.plans.end()) return it->second.get();
     if (D.plans.size() >= PLAN_CACHE_CAP) {
@@ -237,11 +260,12 @@ cudaError_t run_card(CardJob &J) {
     u32 *d_acc = reinterpret_cast<u32 *>(base + J.L.o_acc);
     void *plan_scratch = base + J.L.o_plan;
     const bool multi = J.num_cards > 1;
-    if (multi) J.partials.assign((size_t)J.batches * 32, 0);
+    const u32 PW = cfg.PW, XW = cfg.XW;
+    if (multi) J.partials.assign((size_t)J.batches * XW, 0);
     const u64 part_len = J.L.part_len, card_len = J.L.card_len;
     const bool staged = J.parts > 1;
     const u32 stride = (u32)part_len;  // distance between window tables in a points buffer
-    const size_t point_stage = (size_t)cfg.n_tables * part_len * 16;  // u32 per stage
+    const size_t point_stage = (size_t)cfg.n_tables * part_len * PW;  // u32 per stage
     EventPool events;
 
     // chunk k covers points [k * chunk, ...) of the card range
@@ -258,7 +282,7 @@ cudaError_t run_card(CardJob &J) {
             continue;
         }
         const int mode = multi ? 2 : 0;
-        if (multi) CK(cudaMemsetAsync(d_carry, 0, (size_t)M * 128, st));
+        if (multi) CK(cudaMemsetAsync(d_carry, 0, (size_t)M * XW * 4, st));
         const size_t scalar_stage = (size_t)M * part_len * 8;  // u32 per stage
         cudaEvent_t t0 = nullptr, t1 = nullptr;
         if (cfg.debug) {
@@ -270,8 +294,8 @@ cudaError_t run_card(CardJob &J) {
             // one chunk: upload, then the plain run
             if (!points_resident)
                 for (u32 t = 0; t < cfg.n_tables; t++)
-                    CK(cudaMemcpyAsync(d_points + (size_t)t * part_len * 16, J.h_points[t] + J.L.card_off * 16,
-                                       card_len * 64, cudaMemcpyHostToDevice, st));
+                    CK(cudaMemcpyAsync(d_points + (size_t)t * part_len * PW, J.h_points[t] + J.L.card_off * PW,
+                                       card_len * PW * 4, cudaMemcpyHostToDevice, st));
             points_resident = !staged;
             std::vector<const u32 *> sc(M);
             for (u32 b = 0; b < M; b++) {
@@ -330,11 +354,11 @@ cudaError_t run_card(CardJob &J) {
                 const u32 slot = staged ? k % PART_STAGES : 0;
                 if (staged && k >= PART_STAGES) CK(cudaStreamWaitEvent(cs, computed[k - PART_STAGES], 0));
                 // points of this chunk: staged -> its stage buffer; resident -> in place
-                u32 *pbase = staged ? d_points + slot * point_stage : d_points + s0 * 16;
+                u32 *pbase = staged ? d_points + slot * point_stage : d_points + s0 * PW;
                 if (!points_resident)
                     for (u32 t = 0; t < cfg.n_tables; t++)
-                        CK(cudaMemcpyAsync(pbase + (size_t)t * part_len * 16,
-                                           J.h_points[t] + (J.L.card_off + s0) * 16, mk * 64,
+                        CK(cudaMemcpyAsync(pbase + (size_t)t * part_len * PW,
+                                           J.h_points[t] + (J.L.card_off + s0) * PW, mk * PW * 4,
                                            cudaMemcpyHostToDevice, cs));
                 for (u32 b = 0; b < M; b++) {
                     u32 *dst = staged ? d_scalars + slot * scalar_stage + (size_t)b * part_len * 8
@@ -386,9 +410,10 @@ cudaError_t run_card(CardJob &J) {
         }
         if (!multi) {
             for (u32 b = 0; b < M; b++)
-                CK(cudaMemcpyAsync(J.h_result[g + b], d_results + (size_t)b * 16, 64, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(J.h_result[g + b], d_results + (size_t)b * PW, PW * 4, cudaMemcpyDeviceToHost,
+                                   st));
         } else {
-            CK(cudaMemcpyAsync(J.partials.data() + (size_t)g * 32, d_carry, (size_t)M * 128, cudaMemcpyDeviceToHost,
+            CK(cudaMemcpyAsync(J.partials.data() + (size_t)g * XW, d_carry, (size_t)M * XW * 4, cudaMemcpyDeviceToHost,
                                st));
         }
         CK(cudaStreamSynchronize(st));
@@ -402,8 +427,13 @@ cudaError_t run_card(CardJob &J) {
 extern "C" {
 
 unsigned int impeller_msm_n_precompute(unsigned int window_size, unsigned int target_window) {
+    return impeller_msm_n_precompute_curve(IMPELLER_CURVE_BN254, window_size, target_window);
+}
+
+unsigned int impeller_msm_n_precompute_curve(unsigned int curve, unsigned int window_size,
+                                             unsigned int target_window) {
     Config cfg;
-    if (!make_config(window_size, target_window, 0, cfg)) return 0;
+    if (!make_config(window_size, target_window, 0, cfg, curve)) return 0;
     return cfg.n_tables;
 }
 
@@ -413,10 +443,22 @@ cudaError_t impeller_msm_cfg(unsigned int window_size, unsigned int target_windo
                              unsigned int num_cards, const unsigned int *cards, unsigned int const *const *h_points,
                              unsigned int batches, unsigned int const *const *h_scaler_batch,
                              unsigned int *const *h_result) {
+    return impeller_msm_cfg_curve(IMPELLER_CURVE_BN254, window_size, target_window, debug, buffers, buffer_sizes, len,
+                                  batch_per_run, parts, stage_scalers, stage_points, num_cards, cards, h_points,
+                                  batches, h_scaler_batch, h_result);
+}
+
+cudaError_t impeller_msm_cfg_curve(unsigned int curve, unsigned int window_size, unsigned int target_window,
+                                   int debug, void *const *buffers, unsigned long *buffer_sizes,
+                                   unsigned long long len, unsigned int batch_per_run, unsigned int parts,
+                                   unsigned int stage_scalers, unsigned int stage_points, unsigned int num_cards,
+                                   const unsigned int *cards, unsigned int const *const *h_points,
+                                   unsigned int batches, unsigned int const *const *h_scaler_batch,
+                                   unsigned int *const *h_result) {
     (void)stage_scalers;
     (void)stage_points;
     Config cfg;
-    if (!make_config(window_size, target_window, debug, cfg)) return cudaErrorInvalidValue;
+    if (!make_config(window_size, target_window, debug, cfg, curve)) return cudaErrorInvalidValue;
     if (num_cards == 0 || !cards) {
         set_error("msm: at least one card is required");
         return cudaErrorInvalidValue;
@@ -490,16 +532,17 @@ cudaError_t impeller_msm_cfg(unsigned int window_size, unsigned int target_windo
     cudaStream_t st = device_stream((int)cards[0]);
     unsigned char *base0 = static_cast<unsigned char *>(buffers[0]);
     u32 *d_comb = reinterpret_cast<u32 *>(base0 + layouts[0].o_combine);
-    u32 *d_out = d_comb + (size_t)num_cards * 32;
-    std::vector<u32> gather((size_t)num_cards * 32);
+    const u32 XW = cfg.XW, PW = cfg.PW;
+    u32 *d_out = d_comb + (size_t)num_cards * XW;
+    std::vector<u32> gather((size_t)num_cards * XW);
     for (u32 b = 0; b < batches; b++) {
         for (u32 i = 0; i < num_cards; i++)
-            std::copy(jobs[i].partials.begin() + (size_t)b * 32, jobs[i].partials.begin() + (size_t)(b + 1) * 32,
-                      gather.begin() + (size_t)i * 32);
+            std::copy(jobs[i].partials.begin() + (size_t)b * XW, jobs[i].partials.begin() + (size_t)(b + 1) * XW,
+                      gather.begin() + (size_t)i * XW);
         CK(cudaMemcpyAsync(d_comb, gather.data(), gather.size() * 4, cudaMemcpyHostToDevice, st));
-        cudaError_t e = combine_xyzz(d_comb, num_cards, d_out, st);
+        cudaError_t e = combine_xyzz(d_comb, num_cards, d_out, st, cfg.curve);
         if (e != cudaSuccess) return e;
-        CK(cudaMemcpyAsync(h_result[b], d_out, 64, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(h_result[b], d_out, PW * 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
     }
     return cudaSuccess;
@@ -508,8 +551,16 @@ cudaError_t impeller_msm_cfg(unsigned int window_size, unsigned int target_windo
 cudaError_t impeller_msm_precompute_cfg(unsigned int window_size, unsigned int target_window,
                                         unsigned long long len, unsigned int *const *h_points,
                                         unsigned int max_cards) {
+    return impeller_msm_precompute_cfg_curve(IMPELLER_CURVE_BN254, window_size, target_window, len, h_points,
+                                             max_cards);
+}
+
+cudaError_t impeller_msm_precompute_cfg_curve(unsigned int curve, unsigned int window_size,
+                                              unsigned int target_window, unsigned long long len,
+                                              unsigned int *const *h_points, unsigned int max_cards) {
     Config cfg;
-    if (!make_config(window_size, target_window, 0, cfg)) return cudaErrorInvalidValue;
+    if (!make_config(window_size, target_window, 0, cfg, curve)) return cudaErrorInvalidValue;
+    const u64 PW = cfg.PW;
     if (cfg.n_tables == 1 || len == 0) return cudaSuccess;
     if (!h_points) {
         set_error("msm_precompute: null h_points");
@@ -530,14 +581,14 @@ cudaError_t impeller_msm_precompute_cfg(unsigned int window_size, unsigned int t
         cudaStream_t st = device_stream(dev);
         const u64 chunk = std::min<u64>(cnt, 1ull << 20);
         u32 *d = nullptr;
-        CK(cudaMalloc(&d, (size_t)cfg.n_tables * chunk * 64));
+        CK(cudaMalloc(&d, (size_t)cfg.n_tables * chunk * PW * 4));
         cudaError_t e = cudaSuccess;
         for (u64 s = 0; s < cnt && e == cudaSuccess; s += chunk) {
             const u64 m = std::min<u64>(chunk, cnt - s);
-            e = cudaMemcpyAsync(d, h_points[0] + (off + s) * 16, m * 64, cudaMemcpyHostToDevice, st);
-            if (e == cudaSuccess) e = precompute_tables(d, m, shift, cfg.n_tables, st);
+            e = cudaMemcpyAsync(d, h_points[0] + (off + s) * PW, m * PW * 4, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = precompute_tables(d, m, shift, cfg.n_tables, st, cfg.curve);
             for (u32 t = 1; t < cfg.n_tables && e == cudaSuccess; t++)
-                e = cudaMemcpyAsync(h_points[t] + (off + s) * 16, d + (size_t)t * m * 16, m * 64,
+                e = cudaMemcpyAsync(h_points[t] + (off + s) * PW, d + (size_t)t * m * PW, m * PW * 4,
                                     cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         }

@@ -3,7 +3,8 @@
 //
 // The generator definitions are the ones the CPU oracle uses (splitmix64
 // counter streams; uniform Fr element i = (lo + hi * 2^256) mod r from words
-// 8i..8i+7; the skewed mix; P_i = r_i * G with G = (1, 2)), so the device and
+// 8i..8i+7; the skewed mix; P_i = r_i * G with G the curve's generator:
+// (1, 2) on BN254, the standard G1 generator on BLS12-381), so the device and
 // the oracle produce the same inputs bit for bit.
 #include <string>
 
@@ -11,7 +12,7 @@
 #include "bn254.cuh"
 #include "engine.h"
 
-using namespace bn254;
+using namespace ec;
 
 namespace {
 
@@ -29,39 +30,20 @@ __device__ __forceinline__ u64 stream_key(u64 seed, u64 stream) {
 
 __device__ __forceinline__ u64 stream_word(u64 key, u64 idx) { return mix64(key + (idx + 1) * GAMMA); }
 
-__device__ __forceinline__ bool geq_r(const u32 x[8]) {
-    const u32 m[8] = {FrP::M0, FrP::M1, FrP::M2, FrP::M3, FrP::M4, FrP::M5, FrP::M6, FrP::M7};
-    for (int i = 7; i >= 0; i--)
-        if (x[i] != m[i]) return x[i] > m[i];
-    return true;
-}
-
-__device__ __forceinline__ void sub_r(u32 x[8]) {
-    const u32 m[8] = {FrP::M0, FrP::M1, FrP::M2, FrP::M3, FrP::M4, FrP::M5, FrP::M6, FrP::M7};
-    u64 borrow = 0;
-    for (int i = 0; i < 8; i++) {
-        u64 d = (u64)x[i] - m[i] - borrow;
-        x[i] = (u32)d;
-        borrow = (d >> 63) & 1;
-    }
-}
-
-__device__ __forceinline__ Fr fr_r2() {
-    Fr r;
-    r.l[0] = 0xae216da7u; r.l[1] = 0x1bb8e645u; r.l[2] = 0xe35c59e3u; r.l[3] = 0x53fe3ab1u;
-    r.l[4] = 0x53bb8085u; r.l[5] = 0x8c49833du; r.l[6] = 0x7f4e44a5u; r.l[7] = 0x0216d0b1u;
-    return r;
-}
-
-__device__ __forceinline__ Fq fq_r2() {
-    Fq r;
-    r.l[0] = 0x538afa89u; r.l[1] = 0xf32cfc5bu; r.l[2] = 0xd44501fbu; r.l[3] = 0xb5e71911u;
-    r.l[4] = 0x0a417ff6u; r.l[5] = 0x47ab1effu; r.l[6] = 0xcab8351fu; r.l[7] = 0x06d89f71u;
+template <class F>
+__device__ __forceinline__ Fe<F> fe_rsq() {
+    constexpr Words<F::N> r2 = words(F::RSQ);
+    Fe<F> r;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) r.l[i] = r2.v[i];
     return r;
 }
 
 // canonical uniform Fr element idx of the stream with this key
-__device__ Fr uniform_fr(u64 key, u64 idx) {
+template <class C>
+__device__ Fe<typename C::Fr> uniform_fr(u64 key, u64 idx) {
+    using FR = typename C::Fr;
+    constexpr Words<8> m = words(FR::M);
     u32 lo[8], hi[8];
     for (int k = 0; k < 4; k++) {
         u64 w = stream_word(key, 8 * idx + k);
@@ -71,23 +53,25 @@ __device__ Fr uniform_fr(u64 key, u64 idx) {
         hi[2 * k] = (u32)v;
         hi[2 * k + 1] = (u32)(v >> 32);
     }
-    while (geq_r(lo)) sub_r(lo);
-    while (geq_r(hi)) sub_r(hi);
-    Fr h, l;
+    while (un_geq<8>(lo, m.v)) un_sub<8>(lo, m.v);
+    while (un_geq<8>(hi, m.v)) un_sub<8>(hi, m.v);
+    Fe<FR> h, l;
     for (int i = 0; i < 8; i++) {
         h.l[i] = hi[i];
         l.l[i] = lo[i];
     }
-    Fr t = fe_mul<FrP>(h, fr_r2());  // hi * 2^256 mod r
-    return fe_canon<FrP>(fe_add<FrP>(l, t));
+    Fe<FR> t = fe_mul<FR>(h, fe_rsq<FR>());  // hi * 2^256 mod r
+    return fe_canon<FR>(fe_add<FR>(l, t));
 }
 
+template <class C>
 __global__ void k_gen_scalars(u32 *out, u64 n, u64 seed, u64 stream, int dist, u64 start, int mont) {
+    using FR = typename C::Fr;
     const u64 key = stream_key(seed, stream);
     const u64 key_cat = stream_key(seed, stream + (1ull << 32));
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
         const u64 idx = start + i;
-        Fr v = fe_zero<FrP>();
+        Fe<FR> v = fe_zero<FR>();
         bool uniform = true;
         if (dist == 1) {
             u64 u = stream_word(key_cat, idx);
@@ -98,30 +82,43 @@ __global__ void k_gen_scalars(u32 *out, u64 n, u64 seed, u64 stream, int dist, u
                 else if (cat >= 4) v.l[0] = (u32)((u >> 40) & 0xffffu);
             }
         }
-        if (uniform) v = uniform_fr(key, idx);
-        if (mont) v = fe_canon<FrP>(fe_mul<FrP>(v, fr_r2()));
+        if (uniform) v = uniform_fr<C>(key, idx);
+        if (mont) v = fe_canon<FR>(fe_mul<FR>(v, fe_rsq<FR>()));
         fe_store(out + 8 * i, v);
     }
 }
 
+template <class C>
+__device__ __forceinline__ AffineT<typename C::Fq> generator() {
+    constexpr Words<C::Fq::N> gx = words(C::GX), gy = words(C::GY);
+    AffineT<typename C::Fq> g;
+#pragma unroll
+    for (int i = 0; i < C::Fq::N; i++) {
+        g.x.l[i] = gx.v[i];
+        g.y.l[i] = gy.v[i];
+    }
+    return g;
+}
+
+template <class C>
 __global__ void k_gen_points(u32 *out, u64 n, u64 seed, u64 start) {
+    using FQ = typename C::Fq;
     const u64 key = stream_key(seed, 0);
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        Fr r = uniform_fr(key, start + i);
-        Affine g;
-        g.x = fe_one<FqP>();
-        g.y = fe_add<FqP>(g.x, g.x);
-        Xyzz acc = xyzz_identity();
+        Fe<typename C::Fr> r = uniform_fr<C>(key, start + i);
+        const AffineT<FQ> g = generator<C>();
+        XyzzT<FQ> acc = xyzz_identity<FQ>();
         for (int bit = 255; bit >= 0; bit--) {
             acc = xyzz_dbl(acc);
             if ((r.l[bit >> 5] >> (bit & 31)) & 1u) acc = xyzz_add_affine(acc, g);
         }
-        affine_store(out + 16 * i, xyzz_to_affine(acc));
+        affine_store(out + C::PW * i, xyzz_to_affine(acc));
     }
 }
 
 template <class F>
-__device__ Fe<F> test_op(int op, const Fe<F> &a, const Fe<F> &b, const Fe<F> &r2) {
+__device__ Fe<F> test_op(int op, const Fe<F> &a, const Fe<F> &b) {
+    const Fe<F> r2 = fe_rsq<F>();
     switch (op) {
     case 0: return fe_add<F>(a, b);
     case 1: return fe_sub<F>(a, b);
@@ -136,30 +133,28 @@ __device__ Fe<F> test_op(int op, const Fe<F> &a, const Fe<F> &b, const Fe<F> &r2
     }
 }
 
-__global__ void k_test_field(int field, int op, const u32 *a, const u32 *b, u32 *out, u64 count) {
+template <class F>
+__global__ void k_test_field(int op, const u32 *a, const u32 *b, u32 *out, u64 count) {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    if (field == 0) {
-        Fq x = fe_load<FqP>(a + 8 * i), y = b ? fe_load<FqP>(b + 8 * i) : fe_zero<FqP>();
-        fe_store(out + 8 * i, fe_canon<FqP>(test_op<FqP>(op, x, y, fq_r2())));
-    } else {
-        Fr x = fe_load<FrP>(a + 8 * i), y = b ? fe_load<FrP>(b + 8 * i) : fe_zero<FrP>();
-        fe_store(out + 8 * i, fe_canon<FrP>(test_op<FrP>(op, x, y, fr_r2())));
-    }
+    Fe<F> x = fe_load<F>(a + F::N * i), y = b ? fe_load<F>(b + F::N * i) : fe_zero<F>();
+    fe_store(out + F::N * i, fe_canon<F>(test_op<F>(op, x, y)));
 }
 
+template <class C>
 __global__ void k_test_point(int op, const u32 *p, const u32 *q, u32 *out, u64 count) {
+    using FQ = typename C::Fq;
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    Affine a = affine_load(p + 16 * i);
-    Xyzz r;
+    AffineT<FQ> a = affine_load<FQ>(p + C::PW * i);
+    XyzzT<FQ> r;
     switch (op) {
-    case 0: r = xyzz_add_affine(xyzz_from_affine(a), affine_load(q + 16 * i)); break;
+    case 0: r = xyzz_add_affine(xyzz_from_affine(a), affine_load<FQ>(q + C::PW * i)); break;
     case 1: r = xyzz_dbl(xyzz_from_affine(a)); break;
-    case 2: r = xyzz_add(xyzz_from_affine(a), xyzz_from_affine(affine_load(q + 16 * i))); break;
+    case 2: r = xyzz_add(xyzz_from_affine(a), xyzz_from_affine(affine_load<FQ>(q + C::PW * i))); break;
     default: {
         const u32 *k = q + 8 * i;
-        Xyzz acc = xyzz_identity();
+        XyzzT<FQ> acc = xyzz_identity<FQ>();
         for (int bit = 255; bit >= 0; bit--) {
             acc = xyzz_dbl(acc);
             if ((k[bit >> 5] >> (bit & 31)) & 1u) acc = xyzz_add_affine(acc, a);
@@ -167,7 +162,7 @@ __global__ void k_test_point(int op, const u32 *p, const u32 *q, u32 *out, u64 c
         r = acc;
     }
     }
-    affine_store(out + 16 * i, xyzz_to_affine(r));
+    affine_store(out + C::PW * i, xyzz_to_affine(r));
 }
 
 // Throughput ceiling of the Montgomery product itself: four independent
@@ -232,28 +227,45 @@ cudaError_t launched(const char *what) {
 
 extern "C" {
 
-cudaError_t impeller_gen_scalars(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t stream, int dist,
-                                 uint64_t start, int mont, cudaStream_t s) {
-    if (!d_out && n) {
-        impeller::set_error("impeller_gen_scalars: null output");
+cudaError_t impeller_gen_scalars_curve(int curve, uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t stream,
+                                       int dist, uint64_t start, int mont, cudaStream_t s) {
+    if ((!d_out && n) || (curve != IMPELLER_CURVE_BN254 && curve != IMPELLER_CURVE_BLS12381)) {
+        impeller::set_error("impeller_gen_scalars: bad argument");
         return cudaErrorInvalidValue;
     }
     if (n == 0) return cudaSuccess;
     const u64 blocks = (n + 255) / 256;
-    k_gen_scalars<<<(unsigned)(blocks < 65535 ? blocks : 65535), 256, 0, s>>>(d_out, n, seed, stream, dist, start,
-                                                                               mont);
+    const unsigned grid = (unsigned)(blocks < 65535 ? blocks : 65535);
+    if (curve == IMPELLER_CURVE_BN254)
+        k_gen_scalars<Bn254><<<grid, 256, 0, s>>>(d_out, n, seed, stream, dist, start, mont);
+    else
+        k_gen_scalars<Bls12381><<<grid, 256, 0, s>>>(d_out, n, seed, stream, dist, start, mont);
     return launched("k_gen_scalars");
 }
 
-cudaError_t impeller_gen_points(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t start, cudaStream_t s) {
-    if (!d_out && n) {
-        impeller::set_error("impeller_gen_points: null output");
+cudaError_t impeller_gen_scalars(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t stream, int dist,
+                                 uint64_t start, int mont, cudaStream_t s) {
+    return impeller_gen_scalars_curve(IMPELLER_CURVE_BN254, d_out, n, seed, stream, dist, start, mont, s);
+}
+
+cudaError_t impeller_gen_points_curve(int curve, uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t start,
+                                      cudaStream_t s) {
+    if ((!d_out && n) || (curve != IMPELLER_CURVE_BN254 && curve != IMPELLER_CURVE_BLS12381)) {
+        impeller::set_error("impeller_gen_points: bad argument");
         return cudaErrorInvalidValue;
     }
     if (n == 0) return cudaSuccess;
     const u64 blocks = (n + 127) / 128;
-    k_gen_points<<<(unsigned)(blocks < 65535 ? blocks : 65535), 128, 0, s>>>(d_out, n, seed, start);
+    const unsigned grid = (unsigned)(blocks < 65535 ? blocks : 65535);
+    if (curve == IMPELLER_CURVE_BN254)
+        k_gen_points<Bn254><<<grid, 128, 0, s>>>(d_out, n, seed, start);
+    else
+        k_gen_points<Bls12381><<<grid, 128, 0, s>>>(d_out, n, seed, start);
     return launched("k_gen_points");
+}
+
+cudaError_t impeller_gen_points(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t start, cudaStream_t s) {
+    return impeller_gen_points_curve(IMPELLER_CURVE_BN254, d_out, n, seed, start, s);
 }
 
 cudaError_t impeller_imad_peak(int device, double *gops) {
@@ -310,24 +322,40 @@ cudaError_t impeller_op_latency(int op, uint32_t iters, double *cycles_per_op) {
 
 cudaError_t impeller_test_field_op(int field, int op, const uint32_t *d_a, const uint32_t *d_b, uint32_t *d_out,
                                    uint64_t count, cudaStream_t s) {
-    if (field < 0 || field > 1 || op < 0 || op > 9 || !d_a || !d_out) {
+    if (field < 0 || field > 3 || op < 0 || op > 9 || !d_a || !d_out) {
         impeller::set_error("impeller_test_field_op: bad argument");
         return cudaErrorInvalidValue;
     }
     if (count == 0) return cudaSuccess;
-    k_test_field<<<(unsigned)((count + 127) / 128), 128, 0, s>>>(field, op, d_a, d_b, d_out, count);
+    const unsigned grid = (unsigned)((count + 127) / 128);
+    switch (field) {
+    case 0: k_test_field<FqP><<<grid, 128, 0, s>>>(op, d_a, d_b, d_out, count); break;
+    case 1: k_test_field<FrP><<<grid, 128, 0, s>>>(op, d_a, d_b, d_out, count); break;
+    case 2: k_test_field<BlsFqP><<<grid, 128, 0, s>>>(op, d_a, d_b, d_out, count); break;
+    default: k_test_field<BlsFrP><<<grid, 128, 0, s>>>(op, d_a, d_b, d_out, count); break;
+    }
     return launched("k_test_field");
 }
 
-cudaError_t impeller_test_point_op(int op, const uint32_t *d_p, const uint32_t *d_q, uint32_t *d_out,
-                                   uint64_t count, cudaStream_t s) {
-    if (op < 0 || op > 3 || !d_p || !d_out || (op != 1 && !d_q)) {
+cudaError_t impeller_test_point_op_curve(int curve, int op, const uint32_t *d_p, const uint32_t *d_q, uint32_t *d_out,
+                                         uint64_t count, cudaStream_t s) {
+    if (op < 0 || op > 3 || !d_p || !d_out || (op != 1 && !d_q) ||
+        (curve != IMPELLER_CURVE_BN254 && curve != IMPELLER_CURVE_BLS12381)) {
         impeller::set_error("impeller_test_point_op: bad argument");
         return cudaErrorInvalidValue;
     }
     if (count == 0) return cudaSuccess;
-    k_test_point<<<(unsigned)((count + 127) / 128), 128, 0, s>>>(op, d_p, d_q, d_out, count);
+    const unsigned grid = (unsigned)((count + 127) / 128);
+    if (curve == IMPELLER_CURVE_BN254)
+        k_test_point<Bn254><<<grid, 128, 0, s>>>(op, d_p, d_q, d_out, count);
+    else
+        k_test_point<Bls12381><<<grid, 128, 0, s>>>(op, d_p, d_q, d_out, count);
     return launched("k_test_point");
+}
+
+cudaError_t impeller_test_point_op(int op, const uint32_t *d_p, const uint32_t *d_q, uint32_t *d_out,
+                                   uint64_t count, cudaStream_t s) {
+    return impeller_test_point_op_curve(IMPELLER_CURVE_BN254, op, d_p, d_q, d_out, count, s);
 }
 
 }  // extern "C"

@@ -30,7 +30,7 @@
 
 #include <cstdint>
 
-namespace bn254 {
+namespace ec {
 
 typedef uint32_t u32;
 typedef uint64_t u64;
@@ -45,6 +45,16 @@ struct FqP {
     // 2p
     static constexpr u32 D0 = 0xb0f9fa8eu, D1 = 0x7841182du, D2 = 0xd0e3951au, D3 = 0x2f02d522u;
     static constexpr u32 D4 = 0x0302b0bbu, D5 = 0x70a08b6du, D6 = 0xc2634053u, D7 = 0x60c89ce5u;
+    static constexpr int N = 8;         // limbs
+    static constexpr bool LAZY = true;  // values kept in [0, 2p) (4p < 2^256)
+    static constexpr u32 M[8] = {M0, M1, M2, M3, M4, M5, M6, M7};
+    static constexpr u32 R[8] = {R0, R1, R2, R3, R4, R5, R6, R7};
+    // R^3 mod p (binary inversion)
+    static constexpr u32 RCUBE[8] = {0xda1530dfu, 0xb1cd6dafu, 0xa7283db6u, 0x62f210e6u,
+                                     0x0ada0afbu, 0xef7f0b0cu, 0x2d592544u, 0x20fd6e90u};
+    // R^2 mod p (conversion into Montgomery form)
+    static constexpr u32 RSQ[8] = {0x538afa89u, 0xf32cfc5bu, 0xd44501fbu, 0xb5e71911u,
+                                   0x0a417ff6u, 0x47ab1effu, 0xcab8351fu, 0x06d89f71u};
 };
 
 struct FrP {
@@ -56,12 +66,90 @@ struct FrP {
     // 2r
     static constexpr u32 D0 = 0xe0000002u, D1 = 0x87c3eb27u, D2 = 0xf372e122u, D3 = 0x5067d090u;
     static constexpr u32 D4 = 0x0302b0bau, D5 = 0x70a08b6du, D6 = 0xc2634053u, D7 = 0x60c89ce5u;
+    static constexpr int N = 8;
+    static constexpr bool LAZY = true;  // r < 2^254 as well
+    static constexpr u32 M[8] = {M0, M1, M2, M3, M4, M5, M6, M7};
+    static constexpr u32 R[8] = {R0, R1, R2, R3, R4, R5, R6, R7};
+    static constexpr u32 RSQ[8] = {0xae216da7u, 0x1bb8e645u, 0xe35c59e3u, 0x53fe3ab1u,
+                                   0x53bb8085u, 0x8c49833du, 0x7f4e44a5u, 0x0216d0b1u};
+};
+
+// BLS12-381 scalar field Fr: r < 2^255, so 4r > 2^256 and values stay
+// canonical (every operation reduces fully).  8 limbs like BN254's fields.
+struct BlsFrP {
+    static constexpr u32 M0 = 0x00000001u, M1 = 0xffffffffu, M2 = 0xfffe5bfeu, M3 = 0x53bda402u;
+    static constexpr u32 M4 = 0x09a1d805u, M5 = 0x3339d808u, M6 = 0x299d7d48u, M7 = 0x73eda753u;
+    static constexpr u32 INV = 0xffffffffu;  // -r^{-1} mod 2^32
+    static constexpr u32 R0 = 0xfffffffeu, R1 = 0x00000001u, R2 = 0x00034802u, R3 = 0x5884b7fau;
+    static constexpr u32 R4 = 0xecbc4ff5u, R5 = 0x998c4fefu, R6 = 0xacc5056fu, R7 = 0x1824b159u;
+    static constexpr u32 D0 = 0x00000002u, D1 = 0xfffffffeu, D2 = 0xfffcb7fdu, D3 = 0xa77b4805u;
+    static constexpr u32 D4 = 0x1343b00au, D5 = 0x6673b010u, D6 = 0x533afa90u, D7 = 0xe7db4ea6u;
+    static constexpr int N = 8;
+    static constexpr bool LAZY = false;
+    static constexpr u32 M[8] = {M0, M1, M2, M3, M4, M5, M6, M7};
+    static constexpr u32 R[8] = {R0, R1, R2, R3, R4, R5, R6, R7};
+    static constexpr u32 RSQ[8] = {0xf3f29c6du, 0xc999e990u, 0x87925c23u, 0x2b6cedcbu,
+                                   0x7254398fu, 0x05d31496u, 0x9f59ff11u, 0x0748d9d9u};
+};
+
+// BLS12-381 base field Fq: 381-bit p in 12 limbs; 4p < 2^384, values in [0, 2p).
+struct BlsFqP {
+    static constexpr int N = 12;
+    static constexpr bool LAZY = true;
+    static constexpr u32 INV = 0xfffcfffdu;  // -p^{-1} mod 2^32
+    static constexpr u32 M[12] = {0xffffaaabu, 0xb9feffffu, 0xb153ffffu, 0x1eabfffeu, 0xf6b0f624u, 0x6730d2a0u,
+                                  0xf38512bfu, 0x64774b84u, 0x434bacd7u, 0x4b1ba7b6u, 0x397fe69au, 0x1a0111eau};
+    static constexpr u32 D[12] = {0xffff5556u, 0x73fdffffu, 0x62a7ffffu, 0x3d57fffdu, 0xed61ec48u, 0xce61a541u,
+                                  0xe70a257eu, 0xc8ee9709u, 0x869759aeu, 0x96374f6cu, 0x72ffcd34u, 0x340223d4u};
+    static constexpr u32 R[12] = {0x0002fffdu, 0x76090000u, 0xc40c0002u, 0xebf4000bu, 0x53c758bau, 0x5f489857u,
+                                  0x70525745u, 0x77ce5853u, 0xa256ec6du, 0x5c071a97u, 0xfa80e493u, 0x15f65ec3u};
+    static constexpr u32 RCUBE[12] = {0xd94ca1e0u, 0xed48ac6bu, 0x03a7adf8u, 0x315f831eu, 0x615e29ddu, 0x9a53352au,
+                                      0x921e1761u, 0x34c04e5eu, 0x65724728u, 0x2512d435u, 0x91755d4du, 0x0aa63460u};
+    static constexpr u32 RSQ[12] = {0x1c341746u, 0xf4df1f34u, 0x09d104f1u, 0x0a76e6a6u, 0x4c95b6d5u, 0x8de5476cu,
+                                    0x939d83c0u, 0x67eb88a9u, 0xb519952du, 0x9a793e85u, 0x92cae3aau, 0x11988fe5u};
+};
+
+// Curves: base field, scalar field, affine / XYZZ point words and the
+// generator in Montgomery form.  BN254 G1: y^2 = x^3 + 3, G = (1, 2).
+// BLS12-381 G1: y^2 = x^3 + 4, the standard generator
+// (x = 0x17f1d3a7...db22c6bb, y = 0x08b3f481...46c5e7e1).
+struct Bn254 {
+    using Fq = FqP;
+    using Fr = FrP;
+    static constexpr u32 PW = 16, XW = 32;
+    static constexpr u32 GX[8] = {FqP::R0, FqP::R1, FqP::R2, FqP::R3, FqP::R4, FqP::R5, FqP::R6, FqP::R7};
+    static constexpr u32 GY[8] = {0x8b1e1b3au, 0xa6ba871bu, 0xeb8e167bu, 0x14f1d651u,
+                                  0xf0f28c58u, 0xccdd46deu, 0x340fbe5eu, 0x1c14ef83u};
+};
+struct Bls12381 {
+    using Fq = BlsFqP;
+    using Fr = BlsFrP;
+    static constexpr u32 PW = 24, XW = 48;
+    static constexpr u32 GX[12] = {0xfd530c16u, 0x5cb38790u, 0x9976fff5u, 0x7817fc67u, 0x143ba1c1u, 0x154f95c7u,
+                                   0xf3d0e747u, 0xf0ae6acdu, 0x21dbf440u, 0xedce6eccu, 0x9e0bfb75u, 0x12017741u};
+    static constexpr u32 GY[12] = {0x0ce72271u, 0xbaac93d5u, 0x7918fd8eu, 0x8c22631au, 0x570725ceu, 0xdd595f13u,
+                                   0x50405194u, 0x51ac5829u, 0xad0059c0u, 0x0e1c8c3fu, 0x5008a26au, 0x0bbc3efcu};
 };
 
 template <class F>
 struct Fe {
-    u32 l[8];
+    u32 l[F::N];
 };
+
+// A field constant (F::M, F::R, ...) as a value: device code copies it into
+// a local constexpr with `constexpr Words<F::N> m = words(F::M);` and indexes
+// that (the traits' arrays themselves live in host memory).
+template <int N>
+struct Words {
+    u32 v[N];
+};
+
+template <int N>
+__host__ __device__ constexpr Words<N> words(const u32 (&a)[N]) {
+    Words<N> r{};
+    for (int i = 0; i < N; i++) r.v[i] = a[i];
+    return r;
+}
 
 typedef Fe<FqP> Fq;
 typedef Fe<FrP> Fr;
@@ -70,37 +158,72 @@ template <class F>
 __host__ __device__ __forceinline__ Fe<F> fe_zero() {
     Fe<F> r;
 #pragma unroll
-    for (int i = 0; i < 8; i++) r.l[i] = 0;
+    for (int i = 0; i < F::N; i++) r.l[i] = 0;
     return r;
 }
 
 template <class F>
 __host__ __device__ __forceinline__ Fe<F> fe_one() {
+    constexpr Words<F::N> one = words(F::R);
     Fe<F> r;
-    r.l[0] = F::R0; r.l[1] = F::R1; r.l[2] = F::R2; r.l[3] = F::R3;
-    r.l[4] = F::R4; r.l[5] = F::R5; r.l[6] = F::R6; r.l[7] = F::R7;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) r.l[i] = one.v[i];
+    return r;
+}
+
+// R^3 mod N as a field element (binary inversion).
+template <class F>
+__device__ __forceinline__ Fe<F> fe_rcube() {
+    constexpr Words<F::N> rc = words(F::RCUBE);
+    Fe<F> r;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) r.l[i] = rc.v[i];
     return r;
 }
 
 // Zero test for a canonical value (in [0, N)).
 template <class F>
 __device__ __forceinline__ bool fe_is_zero_canonical(const Fe<F> &a) {
-    u32 x = (a.l[0] | a.l[1]) | (a.l[2] | a.l[3]) | (a.l[4] | a.l[5]) | (a.l[6] | a.l[7]);
+    u32 x = 0;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) x |= a.l[i];
     return x == 0;
 }
 
-// Zero test for a value in [0, 2N): 0 or N.
+// Zero test for a field value: 0 or N in the lazy range [0, 2N).
 template <class F>
 __device__ __forceinline__ bool fe_is_zero(const Fe<F> &a) {
-    u32 x = (a.l[0] | a.l[1]) | (a.l[2] | a.l[3]) | (a.l[4] | a.l[5]) | (a.l[6] | a.l[7]);
-    u32 y = ((a.l[0] ^ F::M0) | (a.l[1] ^ F::M1)) | ((a.l[2] ^ F::M2) | (a.l[3] ^ F::M3)) |
-            ((a.l[4] ^ F::M4) | (a.l[5] ^ F::M5)) | ((a.l[6] ^ F::M6) | (a.l[7] ^ F::M7));
-    return x == 0 || y == 0;
+    if constexpr (!F::LAZY) {
+        return fe_is_zero_canonical(a);
+    } else {
+        constexpr Words<F::N> m = words(F::M);
+        u32 x = 0, y = 0;
+#pragma unroll
+        for (int i = 0; i < F::N; i++) {
+            x |= a.l[i];
+            y |= a.l[i] ^ m.v[i];
+        }
+        return x == 0 || y == 0;
+    }
 }
+
+}  // namespace ec
+
+#include "field12.cuh"
+
+namespace ec {
 
 // r = (t < N) ? t : t - N, for t < 2N.
 template <class F>
-__device__ __forceinline__ void fe_reduce_once(Fe<F> &r, const u32 t[8]) {
+__device__ __forceinline__ void fe_reduce_once(Fe<F> &r, const u32 *t) {
+    if constexpr (F::N == 12) {
+        constexpr Words<12> m = words(F::M);
+        u32 d[12];
+        const u32 bw = sub12(d, t, m.v);
+#pragma unroll
+        for (int i = 0; i < 12; i++) r.l[i] = bw ? t[i] : d[i];
+        return;
+    } else {
     u32 d[8], bw;
     asm("sub.cc.u32  %0, %9, %17;\n\t"
         "subc.cc.u32 %1, %10, %18;\n\t"
@@ -118,11 +241,20 @@ __device__ __forceinline__ void fe_reduce_once(Fe<F> &r, const u32 t[8]) {
     // bw == 0xffffffff when t < N: keep t
 #pragma unroll
     for (int i = 0; i < 8; i++) r.l[i] = bw ? t[i] : d[i];
+    }
 }
 
 // r = (t < 2N) ? t : t - 2N, for t < 4N.
 template <class F>
-__device__ __forceinline__ void fe_reduce_2n(Fe<F> &r, const u32 t[8]) {
+__device__ __forceinline__ void fe_reduce_2n(Fe<F> &r, const u32 *t) {
+    if constexpr (F::N == 12) {
+        constexpr Words<12> d2 = words(F::D);
+        u32 d[12];
+        const u32 bw = sub12(d, t, d2.v);
+#pragma unroll
+        for (int i = 0; i < 12; i++) r.l[i] = bw ? t[i] : d[i];
+        return;
+    } else {
     u32 d[8], bw;
     asm("sub.cc.u32  %0, %9, %17;\n\t"
         "subc.cc.u32 %1, %10, %18;\n\t"
@@ -139,6 +271,7 @@ __device__ __forceinline__ void fe_reduce_2n(Fe<F> &r, const u32 t[8]) {
           "n"(F::D0), "n"(F::D1), "n"(F::D2), "n"(F::D3), "n"(F::D4), "n"(F::D5), "n"(F::D6), "n"(F::D7));
 #pragma unroll
     for (int i = 0; i < 8; i++) r.l[i] = bw ? t[i] : d[i];
+    }
 }
 
 // The canonical representative in [0, N) of a value in [0, 2N).
@@ -232,6 +365,27 @@ __device__ __forceinline__ void bn_row_reduce(u32 (&x)[8], u32 (&y)[8]) {
 // reduction).
 template <class F>
 __device__ __forceinline__ Fe<F> fe_mul_inline(const Fe<F> &a, const Fe<F> &b) {
+    if constexpr (F::N == 12) {
+        u32 u[12], v[12];
+        bn_row_first12(u, v, a.l, b.l[0]);
+        bn_row_reduce12<F>(u, v);
+#pragma unroll
+        for (int i = 1; i < 12; i += 2) {
+            bn_row_next12(v, u, a.l, b.l[i]);
+            bn_row_reduce12<F>(v, u);
+            if (i + 1 < 12) {
+                bn_row_next12(u, v, a.l, b.l[i + 1]);
+                bn_row_reduce12<F>(u, v);
+            }
+        }
+        Fe<F> r;
+        bn_merge12(r.l, u, v);
+        if constexpr (!F::LAZY) {
+            const Fe<F> t = r;
+            fe_reduce_once<F>(r, t.l);
+        }
+        return r;
+    } else {
     u32 u[8], v[8];
     bn_row_first(u, v, a.l, b.l[0]);
     bn_row_reduce<F>(u, v);
@@ -252,7 +406,13 @@ __device__ __forceinline__ Fe<F> fe_mul_inline(const Fe<F> &a, const Fe<F> &b) {
           "=r"(r.l[7])
         : "r"(u[0]), "r"(u[1]), "r"(u[2]), "r"(u[3]), "r"(u[4]), "r"(u[5]), "r"(u[6]), "r"(u[7]), "r"(v[1]),
           "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]));
+    if constexpr (!F::LAZY) {
+        // canonical fields: inputs below N give a result below 2N
+        const Fe<F> t = r;
+        fe_reduce_once<F>(r, t.l);
+    }
     return r;
+    }
 }
 
 // Inlined: with the carries folded into the multiply-adds a product is about
@@ -276,6 +436,12 @@ __device__ __forceinline__ Fe<F> fe_sqr(const Fe<F> &a) {
 // subtraction).
 template <class F>
 __device__ __forceinline__ Fe<F> fe_from_mont(const Fe<F> &a) {
+    if constexpr (F::N == 12) {
+        // a * 1 * R^{-1}: the product with the integer 1, then canonical
+        Fe<F> one_int = fe_zero<F>();
+        one_int.l[0] = 1;
+        return fe_canon<F>(fe_mul_inline<F>(a, one_int));
+    } else {
     u32 t[9];
 #pragma unroll
     for (int i = 0; i < 8; i++) t[i] = a.l[i];
@@ -311,10 +477,19 @@ __device__ __forceinline__ Fe<F> fe_from_mont(const Fe<F> &a) {
     Fe<F> r;
     fe_reduce_once<F>(r, t);
     return r;
+    }
 }
 
 template <class F>
 __device__ __forceinline__ Fe<F> fe_add(const Fe<F> &a, const Fe<F> &b) {
+    if constexpr (F::N == 12) {
+        u32 s[12];
+        add12(s, a.l, b.l);  // a + b < 4N < 2^384
+        Fe<F> r;
+        if constexpr (F::LAZY) fe_reduce_2n<F>(r, s);
+        else fe_reduce_once<F>(r, s);
+        return r;
+    } else {
     u32 s[8];
     asm("add.cc.u32  %0, %8, %16;\n\t"
         "addc.cc.u32 %1, %9, %17;\n\t"
@@ -329,12 +504,23 @@ __device__ __forceinline__ Fe<F> fe_add(const Fe<F> &a, const Fe<F> &b) {
           "r"(a.l[7]), "r"(b.l[0]), "r"(b.l[1]), "r"(b.l[2]), "r"(b.l[3]), "r"(b.l[4]), "r"(b.l[5]),
           "r"(b.l[6]), "r"(b.l[7]));
     Fe<F> r;
-    fe_reduce_2n<F>(r, s);  // a + b < 4N < 2^256
+    // a + b < 4N < 2^256 (lazy) or < 2N (canonical)
+    if constexpr (F::LAZY) fe_reduce_2n<F>(r, s);
+    else fe_reduce_once<F>(r, s);
     return r;
+    }
 }
 
 template <class F>
 __device__ __forceinline__ Fe<F> fe_sub(const Fe<F> &a, const Fe<F> &b) {
+    if constexpr (F::N == 12) {
+        u32 d[12];
+        const u32 bw = sub12(d, a.l, b.l);
+        Fe<F> r;
+        constexpr Words<12> back = F::LAZY ? words(F::D) : words(F::M);
+        add12_masked(r.l, d, back.v, bw);  // add 2N (N) back on borrow
+        return r;
+    } else {
     u32 d[8], bw;
     asm("sub.cc.u32  %0, %9, %17;\n\t"
         "subc.cc.u32 %1, %10, %18;\n\t"
@@ -351,7 +537,10 @@ __device__ __forceinline__ Fe<F> fe_sub(const Fe<F> &a, const Fe<F> &b) {
           "r"(a.l[7]), "r"(b.l[0]), "r"(b.l[1]), "r"(b.l[2]), "r"(b.l[3]), "r"(b.l[4]), "r"(b.l[5]),
           "r"(b.l[6]), "r"(b.l[7]));
     Fe<F> r;
-    // add 2N back when the subtraction borrowed (bw = 0xffffffff)
+    // add 2N (N for canonical fields) back when the subtraction borrowed
+    constexpr u32 k0 = F::LAZY ? F::D0 : F::M0, k1 = F::LAZY ? F::D1 : F::M1, k2 = F::LAZY ? F::D2 : F::M2;
+    constexpr u32 k3 = F::LAZY ? F::D3 : F::M3, k4 = F::LAZY ? F::D4 : F::M4, k5 = F::LAZY ? F::D5 : F::M5;
+    constexpr u32 k6 = F::LAZY ? F::D6 : F::M6, k7 = F::LAZY ? F::D7 : F::M7;
     asm("add.cc.u32  %0, %8, %16;\n\t"
         "addc.cc.u32 %1, %9, %17;\n\t"
         "addc.cc.u32 %2, %10, %18;\n\t"
@@ -363,9 +552,10 @@ __device__ __forceinline__ Fe<F> fe_sub(const Fe<F> &a, const Fe<F> &b) {
         : "=r"(r.l[0]), "=r"(r.l[1]), "=r"(r.l[2]), "=r"(r.l[3]), "=r"(r.l[4]), "=r"(r.l[5]), "=r"(r.l[6]),
           "=r"(r.l[7])
         : "r"(d[0]), "r"(d[1]), "r"(d[2]), "r"(d[3]), "r"(d[4]), "r"(d[5]), "r"(d[6]), "r"(d[7]),
-          "r"(F::D0 & bw), "r"(F::D1 & bw), "r"(F::D2 & bw), "r"(F::D3 & bw), "r"(F::D4 & bw),
-          "r"(F::D5 & bw), "r"(F::D6 & bw), "r"(F::D7 & bw));
+          "r"(k0 & bw), "r"(k1 & bw), "r"(k2 & bw), "r"(k3 & bw), "r"(k4 & bw), "r"(k5 & bw), "r"(k6 & bw),
+          "r"(k7 & bw));
     return r;
+    }
 }
 
 template <class F>
@@ -378,9 +568,9 @@ __device__ __forceinline__ Fe<F> fe_dbl(const Fe<F> &a) {
     return fe_add<F>(a, a);
 }
 
-// a^e for a plain exponent given as 8 little-endian limbs, 4-bit fixed window.
+// a^e for a plain exponent given as F::N little-endian limbs, 4-bit fixed window.
 template <class F>
-__device__ __noinline__ Fe<F> fe_pow(const Fe<F> &a, const u32 e[8]) {
+__device__ __noinline__ Fe<F> fe_pow(const Fe<F> &a, const u32 *e) {
     Fe<F> tab[16];
     tab[0] = fe_one<F>();
     tab[1] = a;
@@ -388,7 +578,7 @@ __device__ __noinline__ Fe<F> fe_pow(const Fe<F> &a, const u32 e[8]) {
     for (int i = 2; i < 16; i++) tab[i] = fe_mul<F>(tab[i - 1], a);
     Fe<F> acc = fe_one<F>();
 #pragma unroll 1
-    for (int nib = 63; nib >= 0; nib--) {
+    for (int nib = 8 * F::N - 1; nib >= 0; nib--) {
         acc = fe_sqr<F>(acc);
         acc = fe_sqr<F>(acc);
         acc = fe_sqr<F>(acc);
@@ -407,7 +597,14 @@ __device__ __noinline__ Fe<F> fe_pow(const Fe<F> &a, const u32 e[8]) {
 // Fermat inversion a^(N-2); inverse of zero is zero.
 template <class F>
 __device__ __forceinline__ Fe<F> fe_inv(const Fe<F> &a) {
-    u32 e[8] = {F::M0 - 2u, F::M1, F::M2, F::M3, F::M4, F::M5, F::M6, F::M7};
+    constexpr Words<F::N> m = words(F::M);
+    u32 e[F::N];
+    u32 borrow = 2;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) {
+        e[i] = m.v[i] - borrow;
+        borrow = m.v[i] < borrow ? 1u : 0u;
+    }
     return fe_pow<F>(a, e);
 }
 
@@ -417,40 +614,71 @@ __device__ __forceinline__ Fe<F> fe_inv(const Fe<F> &a) {
 // product with R^3 mod N turns it into A^{-1} R.  Variable time (the inputs
 // are public).  Inverse of zero is zero.  The loop is bounded: every step
 // shrinks u + v by at least one bit.
-template <class F>
-__device__ __forceinline__ bool u256_is_one(const u32 x[8]) {
-    return x[0] == 1 && (x[1] | x[2] | x[3] | x[4] | x[5] | x[6] | x[7]) == 0;
-}
-
-__device__ __forceinline__ void u256_shr1(u32 x[8], u32 top) {
+template <int N>
+__device__ __forceinline__ bool un_is_one(const u32 *x) {
+    u32 o = x[0] ^ 1u;
 #pragma unroll
-    for (int i = 0; i < 7; i++) x[i] = __funnelshift_r(x[i], x[i + 1], 1);
-    x[7] = (x[7] >> 1) | (top << 31);
+    for (int i = 1; i < N; i++) o |= x[i];
+    return o == 0;
 }
 
-__device__ __forceinline__ bool u256_geq(const u32 a[8], const u32 b[8]) {
-    for (int i = 7; i >= 0; i--)
+template <int N>
+__device__ __forceinline__ bool un_is_zero(const u32 *x) {
+    u32 o = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) o |= x[i];
+    return o == 0;
+}
+
+template <int N>
+__device__ __forceinline__ void un_shr1(u32 *x, u32 top) {
+#pragma unroll
+    for (int i = 0; i < N - 1; i++) x[i] = __funnelshift_r(x[i], x[i + 1], 1);
+    x[N - 1] = (x[N - 1] >> 1) | (top << 31);
+}
+
+template <int N>
+__device__ __forceinline__ bool un_geq(const u32 *a, const u32 *b) {
+    for (int i = N - 1; i >= 0; i--)
         if (a[i] != b[i]) return a[i] > b[i];
     return true;
 }
 
-__device__ __forceinline__ void u256_sub(u32 a[8], const u32 b[8]) {
-    asm("sub.cc.u32  %0, %0, %8;\n\t"
-        "subc.cc.u32 %1, %1, %9;\n\t"
-        "subc.cc.u32 %2, %2, %10;\n\t"
-        "subc.cc.u32 %3, %3, %11;\n\t"
-        "subc.cc.u32 %4, %4, %12;\n\t"
-        "subc.cc.u32 %5, %5, %13;\n\t"
-        "subc.cc.u32 %6, %6, %14;\n\t"
-        "subc.u32    %7, %7, %15;"
-        : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7])
-        : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+// a -= b (no borrow out: callers subtract the smaller value)
+template <int N>
+__device__ __forceinline__ void un_sub(u32 *a, const u32 *b) {
+    if constexpr (N == 12) {
+        u32 d[12];
+        sub12(d, a, b);
+#pragma unroll
+        for (int i = 0; i < 12; i++) a[i] = d[i];
+    } else {
+        asm("sub.cc.u32  %0, %0, %8;\n\t"
+            "subc.cc.u32 %1, %1, %9;\n\t"
+            "subc.cc.u32 %2, %2, %10;\n\t"
+            "subc.cc.u32 %3, %3, %11;\n\t"
+            "subc.cc.u32 %4, %4, %12;\n\t"
+            "subc.cc.u32 %5, %5, %13;\n\t"
+            "subc.cc.u32 %6, %6, %14;\n\t"
+            "subc.u32    %7, %7, %15;"
+            : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7])
+            : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+    }
 }
 
 // x = x / 2 mod N for x < 2N (N odd): if x is odd, (x + N) / 2 < 3N / 2.
 template <class F>
-__device__ __forceinline__ void fe_half(u32 x[8]) {
-    if (x[0] & 1u) {
+__device__ __forceinline__ void fe_half(u32 *x) {
+    if constexpr (F::N == 12) {
+        if (x[0] & 1u) {
+            constexpr Words<12> m = words(F::M);
+            u32 t[12];
+            add12(t, x, m.v);  // x + N < 3N < 2^384
+#pragma unroll
+            for (int i = 0; i < 12; i++) x[i] = t[i];
+        }
+        un_shr1<12>(x, 0);
+    } else if (x[0] & 1u) {
         u32 c;
         asm("add.cc.u32  %0, %0, %9;\n\t"
             "addc.cc.u32 %1, %1, %10;\n\t"
@@ -464,9 +692,9 @@ __device__ __forceinline__ void fe_half(u32 x[8]) {
             : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]), "+r"(x[7]),
               "=r"(c)
             : "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5), "n"(F::M6), "n"(F::M7));
-        u256_shr1(x, c);
+        un_shr1<8>(x, c);
     } else {
-        u256_shr1(x, 0);
+        un_shr1<8>(x, 0);
     }
 }
 
@@ -474,116 +702,139 @@ template <class F>
 __device__ __noinline__ Fe<F> fe_inv_binary(const Fe<F> &a_in, const Fe<F> &r3) {
     const Fe<F> a = fe_canon<F>(a_in);
     if (fe_is_zero_canonical(a)) return a;
-    u32 u[8], v[8];
+    constexpr int N = F::N;
+    constexpr Words<N> m = words(F::M);
+    u32 u[N], v[N];
     Fe<F> x1 = fe_zero<F>(), x2 = fe_zero<F>();
     x1.l[0] = 1;
 #pragma unroll
-    for (int i = 0; i < 8; i++) u[i] = a.l[i];
-    v[0] = F::M0; v[1] = F::M1; v[2] = F::M2; v[3] = F::M3;
-    v[4] = F::M4; v[5] = F::M5; v[6] = F::M6; v[7] = F::M7;
+    for (int i = 0; i < N; i++) {
+        u[i] = a.l[i];
+        v[i] = m.v[i];
+    }
     // One shift or one subtraction per step; a valid input (0 < a < N, N
-    // prime) needs at most ~4 * 254 steps.  The zero check and the step bound
-    // keep a non-canonical input from looping: it yields zero.
+    // prime) needs at most ~4 * log2 N steps.  The zero check and the step
+    // bound keep a non-canonical input from looping: it yields zero.
     bool done = false;
     for (int step = 0; step < 4096; step++) {
-        if (u256_is_one<F>(u) || u256_is_one<F>(v)) {
+        if (un_is_one<N>(u) || un_is_one<N>(v)) {
             done = true;
             break;
         }
-        if ((u[0] | u[1] | u[2] | u[3] | u[4] | u[5] | u[6] | u[7]) == 0 ||
-            (v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7]) == 0)
-            break;
+        if (un_is_zero<N>(u) || un_is_zero<N>(v)) break;
         if (!(u[0] & 1u)) {
-            u256_shr1(u, 0);
+            un_shr1<N>(u, 0);
             fe_half<F>(x1.l);
         } else if (!(v[0] & 1u)) {
-            u256_shr1(v, 0);
+            un_shr1<N>(v, 0);
             fe_half<F>(x2.l);
-        } else if (u256_geq(u, v)) {
-            u256_sub(u, v);
+        } else if (un_geq<N>(u, v)) {
+            un_sub<N>(u, v);
             x1 = fe_sub<F>(x1, x2);
         } else {
-            u256_sub(v, u);
+            un_sub<N>(v, u);
             x2 = fe_sub<F>(x2, x1);
         }
     }
     if (!done) return fe_zero<F>();
-    return fe_mul<F>(u256_is_one<F>(u) ? x1 : x2, r3);
+    return fe_mul<F>(un_is_one<N>(u) ? x1 : x2, r3);
 }
 
+// 16-byte vector loads and stores (element addresses are 16-byte aligned).
 template <class F>
 __device__ __forceinline__ Fe<F> fe_load(const u32 *p) {
     Fe<F> r;
     const uint4 *q = reinterpret_cast<const uint4 *>(p);
-    uint4 lo = q[0], hi = q[1];
-    r.l[0] = lo.x; r.l[1] = lo.y; r.l[2] = lo.z; r.l[3] = lo.w;
-    r.l[4] = hi.x; r.l[5] = hi.y; r.l[6] = hi.z; r.l[7] = hi.w;
+#pragma unroll
+    for (int k = 0; k < F::N / 4; k++) {
+        const uint4 v = q[k];
+        r.l[4 * k] = v.x;
+        r.l[4 * k + 1] = v.y;
+        r.l[4 * k + 2] = v.z;
+        r.l[4 * k + 3] = v.w;
+    }
     return r;
 }
 
 template <class F>
 __device__ __forceinline__ void fe_store(u32 *p, const Fe<F> &a) {
     uint4 *q = reinterpret_cast<uint4 *>(p);
-    q[0] = make_uint4(a.l[0], a.l[1], a.l[2], a.l[3]);
-    q[1] = make_uint4(a.l[4], a.l[5], a.l[6], a.l[7]);
+#pragma unroll
+    for (int k = 0; k < F::N / 4; k++) q[k] = make_uint4(a.l[4 * k], a.l[4 * k + 1], a.l[4 * k + 2], a.l[4 * k + 3]);
 }
 
-// ---------------------------------------------------------------- G1 (XYZZ)
+// ----------------------------------------------------------- G1 (XYZZ)
+//
+// Templates over the base field F: BN254 G1 (F = FqP, 16-word affine, 32-word
+// XYZZ) and BLS12-381 G1 (F = BlsFqP, 24 / 48 words).  Both curves are
+// y^2 = x^3 + b with a = 0, the case the formulas below are written for.
 
-struct Affine {
-    Fq x, y;
+template <class F>
+struct AffineT {
+    Fe<F> x, y;
 };
 
-struct Xyzz {
-    Fq x, y, zz, zzz;
+template <class F>
+struct XyzzT {
+    Fe<F> x, y, zz, zzz;
 };
+
+typedef AffineT<FqP> Affine;
+typedef XyzzT<FqP> Xyzz;
 
 // Affine points come from memory in canonical form; negation keeps 0 at 0.
-__device__ __forceinline__ bool affine_is_identity(const Affine &a) { return fe_is_zero_canonical(a.y); }
+template <class F>
+__device__ __forceinline__ bool affine_is_identity(const AffineT<F> &a) { return fe_is_zero_canonical(a.y); }
 
-__device__ __forceinline__ Xyzz xyzz_identity() {
-    Xyzz r;
-    r.x = fe_zero<FqP>();
-    r.y = fe_zero<FqP>();
-    r.zz = fe_zero<FqP>();
-    r.zzz = fe_zero<FqP>();
+template <class F = FqP>
+__device__ __forceinline__ XyzzT<F> xyzz_identity() {
+    XyzzT<F> r;
+    r.x = fe_zero<F>();
+    r.y = fe_zero<F>();
+    r.zz = fe_zero<F>();
+    r.zzz = fe_zero<F>();
     return r;
 }
 
-__device__ __forceinline__ bool xyzz_is_identity(const Xyzz &p) { return fe_is_zero(p.zz); }
+template <class F>
+__device__ __forceinline__ bool xyzz_is_identity(const XyzzT<F> &p) { return fe_is_zero(p.zz); }
 
-__device__ __forceinline__ Xyzz xyzz_from_affine(const Affine &a) {
-    if (affine_is_identity(a)) return xyzz_identity();
-    Xyzz r;
+template <class F>
+__device__ __forceinline__ XyzzT<F> xyzz_from_affine(const AffineT<F> &a) {
+    if (affine_is_identity(a)) return xyzz_identity<F>();
+    XyzzT<F> r;
     r.x = a.x;
     r.y = a.y;
-    r.zz = fe_one<FqP>();
+    r.zz = fe_one<F>();
     r.zzz = r.zz;
     return r;
 }
 
-__device__ __forceinline__ Affine affine_neg(const Affine &a) {
-    Affine r;
+template <class F>
+__device__ __forceinline__ AffineT<F> affine_neg(const AffineT<F> &a) {
+    AffineT<F> r;
     r.x = a.x;
-    r.y = fe_neg<FqP>(a.y);
+    r.y = fe_neg<F>(a.y);
     return r;
 }
 
-__device__ __forceinline__ Xyzz xyzz_neg(const Xyzz &p) {
-    Xyzz r = p;
-    r.y = fe_neg<FqP>(p.y);
+template <class F>
+__device__ __forceinline__ XyzzT<F> xyzz_neg(const XyzzT<F> &p) {
+    XyzzT<F> r = p;
+    r.y = fe_neg<F>(p.y);
     return r;
 }
 
 // mdbl-2008-s-1: 2*a for an affine, non-identity a.
-__device__ __forceinline__ Xyzz affine_dbl(const Affine &a) {
-    Fq u = fe_dbl(a.y);
-    Fq v = fe_sqr(u);
-    Fq w = fe_mul(u, v);
-    Fq s = fe_mul(a.x, v);
-    Fq x2 = fe_sqr(a.x);
-    Fq m = fe_add(fe_dbl(x2), x2);
-    Xyzz r;
+template <class F>
+__device__ __forceinline__ XyzzT<F> affine_dbl(const AffineT<F> &a) {
+    Fe<F> u = fe_dbl(a.y);
+    Fe<F> v = fe_sqr(u);
+    Fe<F> w = fe_mul(u, v);
+    Fe<F> s = fe_mul(a.x, v);
+    Fe<F> x2 = fe_sqr(a.x);
+    Fe<F> m = fe_add(fe_dbl(x2), x2);
+    XyzzT<F> r;
     r.x = fe_sub(fe_sub(fe_sqr(m), s), s);
     r.y = fe_sub(fe_mul(m, fe_sub(s, r.x)), fe_mul(w, a.y));
     r.zz = v;
@@ -592,15 +843,16 @@ __device__ __forceinline__ Xyzz affine_dbl(const Affine &a) {
 }
 
 // dbl-2008-s-1 with a = 0.
-__device__ __forceinline__ Xyzz xyzz_dbl(const Xyzz &p) {
+template <class F>
+__device__ __forceinline__ XyzzT<F> xyzz_dbl(const XyzzT<F> &p) {
     if (xyzz_is_identity(p)) return p;
-    Fq u = fe_dbl(p.y);
-    Fq v = fe_sqr(u);
-    Fq w = fe_mul(u, v);
-    Fq s = fe_mul(p.x, v);
-    Fq x2 = fe_sqr(p.x);
-    Fq m = fe_add(fe_dbl(x2), x2);
-    Xyzz r;
+    Fe<F> u = fe_dbl(p.y);
+    Fe<F> v = fe_sqr(u);
+    Fe<F> w = fe_mul(u, v);
+    Fe<F> s = fe_mul(p.x, v);
+    Fe<F> x2 = fe_sqr(p.x);
+    Fe<F> m = fe_add(fe_dbl(x2), x2);
+    XyzzT<F> r;
     r.x = fe_sub(fe_sub(fe_sqr(m), s), s);
     r.y = fe_sub(fe_mul(m, fe_sub(s, r.x)), fe_mul(w, p.y));
     r.zz = fe_mul(v, p.zz);
@@ -609,129 +861,129 @@ __device__ __forceinline__ Xyzz xyzz_dbl(const Xyzz &p) {
 }
 
 // madd-2008-s: p + q, q affine.  Handles every special case.
-__device__ __forceinline__ Xyzz xyzz_add_affine(const Xyzz &p, const Affine &q) {
+template <class F>
+__device__ __forceinline__ XyzzT<F> xyzz_add_affine(const XyzzT<F> &p, const AffineT<F> &q) {
     if (affine_is_identity(q)) return p;
     if (xyzz_is_identity(p)) return xyzz_from_affine(q);
-    Fq u2 = fe_mul(q.x, p.zz);
-    Fq s2 = fe_mul(q.y, p.zzz);
-    Fq P = fe_sub(u2, p.x);
-    Fq R = fe_sub(s2, p.y);
+    Fe<F> u2 = fe_mul(q.x, p.zz);
+    Fe<F> s2 = fe_mul(q.y, p.zzz);
+    Fe<F> P = fe_sub(u2, p.x);
+    Fe<F> R = fe_sub(s2, p.y);
     if (fe_is_zero(P)) {
         if (fe_is_zero(R)) return affine_dbl(q);
-        return xyzz_identity();
+        return xyzz_identity<F>();
     }
-    Fq pp = fe_sqr(P);
-    Fq ppp = fe_mul(P, pp);
-    Fq Q = fe_mul(p.x, pp);
-    Xyzz r;
+    Fe<F> pp = fe_sqr(P);
+    Fe<F> ppp = fe_mul(P, pp);
+    Fe<F> Q = fe_mul(p.x, pp);
+    XyzzT<F> r;
     r.zz = fe_mul(p.zz, pp);
     r.zzz = fe_mul(p.zzz, ppp);
-    Fq t = fe_mul(p.y, ppp);
+    Fe<F> t = fe_mul(p.y, ppp);
     r.x = fe_sub(fe_sub(fe_sub(fe_sqr(R), ppp), Q), Q);
     r.y = fe_sub(fe_mul(R, fe_sub(Q, r.x)), t);
     return r;
 }
 
 // add-2008-s: p + q.  Handles every special case.
-__device__ __forceinline__ Xyzz xyzz_add(const Xyzz &p, const Xyzz &q) {
+template <class F>
+__device__ __forceinline__ XyzzT<F> xyzz_add(const XyzzT<F> &p, const XyzzT<F> &q) {
     if (xyzz_is_identity(p)) return q;
     if (xyzz_is_identity(q)) return p;
-    Fq u1 = fe_mul(p.x, q.zz);
-    Fq u2 = fe_mul(q.x, p.zz);
-    Fq s1 = fe_mul(p.y, q.zzz);
-    Fq s2 = fe_mul(q.y, p.zzz);
-    Fq P = fe_sub(u2, u1);
-    Fq R = fe_sub(s2, s1);
+    Fe<F> u1 = fe_mul(p.x, q.zz);
+    Fe<F> u2 = fe_mul(q.x, p.zz);
+    Fe<F> s1 = fe_mul(p.y, q.zzz);
+    Fe<F> s2 = fe_mul(q.y, p.zzz);
+    Fe<F> P = fe_sub(u2, u1);
+    Fe<F> R = fe_sub(s2, s1);
     if (fe_is_zero(P)) {
         if (fe_is_zero(R)) return xyzz_dbl(p);
-        return xyzz_identity();
+        return xyzz_identity<F>();
     }
-    Fq pp = fe_sqr(P);
-    Fq ppp = fe_mul(P, pp);
-    Fq Q = fe_mul(u1, pp);
-    Xyzz r;
+    Fe<F> pp = fe_sqr(P);
+    Fe<F> ppp = fe_mul(P, pp);
+    Fe<F> Q = fe_mul(u1, pp);
+    XyzzT<F> r;
     r.zz = fe_mul(fe_mul(p.zz, q.zz), pp);
     r.zzz = fe_mul(fe_mul(p.zzz, q.zzz), ppp);
-    Fq t = fe_mul(s1, ppp);
+    Fe<F> t = fe_mul(s1, ppp);
     r.x = fe_sub(fe_sub(fe_sub(fe_sqr(R), ppp), Q), Q);
     r.y = fe_sub(fe_mul(R, fe_sub(Q, r.x)), t);
     return r;
 }
 
-__device__ __forceinline__ Fq fq_r3() {
-    Fq r;  // R^3 mod p
-    r.l[0] = 0xda1530dfu; r.l[1] = 0xb1cd6dafu; r.l[2] = 0xa7283db6u; r.l[3] = 0x62f210e6u;
-    r.l[4] = 0x0ada0afbu; r.l[5] = 0xef7f0b0cu; r.l[6] = 0x2d592544u; r.l[7] = 0x20fd6e90u;
-    return r;
-}
+__device__ __forceinline__ Fq fq_r3() { return fe_rcube<FqP>(); }
 
 // Canonical affine form; identity -> (0, 0).  Latency-optimised (binary
 // inversion): used once per MSM result.
-__device__ __forceinline__ Affine xyzz_to_affine_fast(const Xyzz &p) {
-    Affine r;
+template <class F>
+__device__ __forceinline__ AffineT<F> xyzz_to_affine_fast(const XyzzT<F> &p) {
+    AffineT<F> r;
     if (xyzz_is_identity(p)) {
-        r.x = fe_zero<FqP>();
-        r.y = fe_zero<FqP>();
+        r.x = fe_zero<F>();
+        r.y = fe_zero<F>();
         return r;
     }
-    Fq a = fe_inv_binary<FqP>(p.zzz, fq_r3());
-    Fq b = fe_sqr(fe_mul(p.zz, a));
+    Fe<F> a = fe_inv_binary<F>(p.zzz, fe_rcube<F>());
+    Fe<F> b = fe_sqr(fe_mul(p.zz, a));
     r.x = fe_canon(fe_mul(p.x, b));
     r.y = fe_canon(fe_mul(p.y, a));
     return r;
 }
 
 // Canonical affine form; identity -> (0, 0).
-__device__ __forceinline__ Affine xyzz_to_affine(const Xyzz &p) {
-    Affine r;
+template <class F>
+__device__ __forceinline__ AffineT<F> xyzz_to_affine(const XyzzT<F> &p) {
+    AffineT<F> r;
     if (xyzz_is_identity(p)) {
-        r.x = fe_zero<FqP>();
-        r.y = fe_zero<FqP>();
+        r.x = fe_zero<F>();
+        r.y = fe_zero<F>();
         return r;
     }
-    Fq a = fe_inv(p.zzz);
-    Fq b = fe_sqr(fe_mul(p.zz, a));
+    Fe<F> a = fe_inv(p.zzz);
+    Fe<F> b = fe_sqr(fe_mul(p.zz, a));
     r.x = fe_canon(fe_mul(p.x, b));
     r.y = fe_canon(fe_mul(p.y, a));
     return r;
 }
 
-__device__ __forceinline__ Affine affine_load(const u32 *p) {
-    Affine a;
-    const uint4 *q = reinterpret_cast<const uint4 *>(p);
-    uint4 v0 = q[0], v1 = q[1], v2 = q[2], v3 = q[3];
-    a.x.l[0] = v0.x; a.x.l[1] = v0.y; a.x.l[2] = v0.z; a.x.l[3] = v0.w;
-    a.x.l[4] = v1.x; a.x.l[5] = v1.y; a.x.l[6] = v1.z; a.x.l[7] = v1.w;
-    a.y.l[0] = v2.x; a.y.l[1] = v2.y; a.y.l[2] = v2.z; a.y.l[3] = v2.w;
-    a.y.l[4] = v3.x; a.y.l[5] = v3.y; a.y.l[6] = v3.z; a.y.l[7] = v3.w;
+template <class F = FqP>
+__device__ __forceinline__ AffineT<F> affine_load(const u32 *p) {
+    AffineT<F> a;
+    a.x = fe_load<F>(p);
+    a.y = fe_load<F>(p + F::N);
     return a;
 }
 
-__device__ __forceinline__ void affine_store(u32 *p, const Affine &a) {
+template <class F>
+__device__ __forceinline__ void affine_store(u32 *p, const AffineT<F> &a) {
     fe_store(p, a.x);
-    fe_store(p + 8, a.y);
+    fe_store(p + F::N, a.y);
 }
 
-__device__ __forceinline__ Xyzz xyzz_load(const u32 *p) {
-    Xyzz r;
-    r.x = fe_load<FqP>(p);
-    r.y = fe_load<FqP>(p + 8);
-    r.zz = fe_load<FqP>(p + 16);
-    r.zzz = fe_load<FqP>(p + 24);
+template <class F = FqP>
+__device__ __forceinline__ XyzzT<F> xyzz_load(const u32 *p) {
+    XyzzT<F> r;
+    r.x = fe_load<F>(p);
+    r.y = fe_load<F>(p + F::N);
+    r.zz = fe_load<F>(p + 2 * F::N);
+    r.zzz = fe_load<F>(p + 3 * F::N);
     return r;
 }
 
-__device__ __forceinline__ void xyzz_store(u32 *p, const Xyzz &a) {
+template <class F>
+__device__ __forceinline__ void xyzz_store(u32 *p, const XyzzT<F> &a) {
     fe_store(p, a.x);
-    fe_store(p + 8, a.y);
-    fe_store(p + 16, a.zz);
-    fe_store(p + 24, a.zzz);
+    fe_store(p + F::N, a.y);
+    fe_store(p + 2 * F::N, a.zz);
+    fe_store(p + 3 * F::N, a.zzz);
 }
 
-__device__ __forceinline__ Xyzz xyzz_shfl_down(const Xyzz &p, u32 delta, u32 mask = 0xffffffffu) {
-    Xyzz r;
+template <class F>
+__device__ __forceinline__ XyzzT<F> xyzz_shfl_down(const XyzzT<F> &p, u32 delta, u32 mask = 0xffffffffu) {
+    XyzzT<F> r;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < F::N; i++) {
         r.x.l[i] = __shfl_down_sync(mask, p.x.l[i], delta);
         r.y.l[i] = __shfl_down_sync(mask, p.y.l[i], delta);
         r.zz.l[i] = __shfl_down_sync(mask, p.zz.l[i], delta);
@@ -741,8 +993,9 @@ __device__ __forceinline__ Xyzz xyzz_shfl_down(const Xyzz &p, u32 delta, u32 mas
 }
 
 // k * p for a small plain scalar k, left-to-right double-and-add.
-__device__ __forceinline__ Xyzz xyzz_mul_u32(const Xyzz &p, u32 k) {
-    Xyzz acc = xyzz_identity();
+template <class F>
+__device__ __forceinline__ XyzzT<F> xyzz_mul_u32(const XyzzT<F> &p, u32 k) {
+    XyzzT<F> acc = xyzz_identity<F>();
     if (k == 0) return acc;
     int top = 31 - __clz(k);
 #pragma unroll 1
@@ -753,4 +1006,4 @@ __device__ __forceinline__ Xyzz xyzz_mul_u32(const Xyzz &p, u32 k) {
     return acc;
 }
 
-}  // namespace bn254
+}  // namespace ec

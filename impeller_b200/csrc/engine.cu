@@ -15,6 +15,8 @@
 
 namespace impeller {
 
+typedef uint8_t u8;
+
 static thread_local std::string g_err;
 
 void set_error(const std::string &msg) { g_err = msg; }
@@ -38,7 +40,24 @@ const char *last_error() { return g_err.c_str(); }
         }                                                                                       \
     } while (0)
 
-u32 digit_windows(u32 c) { return (254u + c - 1u) / c; }
+u32 digit_windows(u32 c, u32 curve) {
+    if (curve == CURVE_BLS12381) {
+        // smallest W with ((r - 1) >> (c (W - 1))) + 1 <= 2^(c - 1), r the BLS12-381 group order
+        static const u8 bls[32] = {0,  0,  0,  86, 64, 52, 43, 37, 32, 29, 26, 24, 22, 20, 19, 18,
+                                   16, 16, 15, 14, 13, 13, 12, 12, 11, 11, 10, 10, 10, 9,  9,  9};
+        return c < 32 ? bls[c] : 0;
+    }
+    return (254u + c - 1u) / c;
+}
+
+// Launch `kern` instantiated for the plan's curve.
+#define CURVE_LAUNCH(curve_id, kern, grid, block, smem, st, ...)                      \
+    do {                                                                               \
+        if ((curve_id) == CURVE_BLS12381)                                              \
+            kern<Bls12381><<<(grid), (block), (smem), (st)>>>(__VA_ARGS__);            \
+        else                                                                           \
+            kern<Bn254><<<(grid), (block), (smem), (st)>>>(__VA_ARGS__);               \
+    } while (0)
 
 int sm_count(int device) {
     static std::mutex mu;
@@ -63,6 +82,17 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
         return false;
     }
     const int sms = sm_count(device);
+    p.curve = shapes[0].curve;
+    if (p.curve != CURVE_BN254 && p.curve != CURVE_BLS12381) {
+        set_error("unknown curve");
+        return false;
+    }
+    for (const MsmShape &sh : shapes)
+        if (sh.curve != p.curve) {
+            set_error("every MSM of a plan must be on the same curve");
+            return false;
+        }
+    const size_t XB = (size_t)xyzz_words(p.curve) * 4, PB = (size_t)point_words(p.curve) * 4;
     std::vector<MsmDesc> descs(p.M);
     std::vector<WinDesc> wins;
     u64 nb = 0, entries = 0;
@@ -73,7 +103,7 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
             set_error("window size must be in [3, 31]");
             return false;
         }
-        const u32 W = digit_windows(s.c);
+        const u32 W = digit_windows(s.c, p.curve);
         const u32 nw = (s.n_windows == 0 || s.n_windows > W) ? W : s.n_windows;
         const u32 n_tables = (W + nw - 1) / nw;
         const u64 B = 1ull << (s.c - 1);
@@ -229,15 +259,15 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     lo.o_nsegs = take(p.msd ? 4 : 0);
     lo.o_seghist = take(p.msd ? (size_t)p.segcap * FINE * 4 : 0);
     lo.o_segcur = take(p.msd ? (size_t)p.segcap * FINE * 4 : 0);
-    lo.o_buckets = take((size_t)p.nb * 128);
+    lo.o_buckets = take((size_t)p.nb * XB);
     lo.o_recb = take((size_t)2 * T * 4);
-    lo.o_recp = take((size_t)2 * T * 128);
-    lo.o_parts = take((size_t)nparts * 128);
-    lo.o_parts_s = take((size_t)nparts * 128);
-    lo.o_wres = take((size_t)wins.size() * 128);
+    lo.o_recp = take((size_t)2 * T * XB);
+    lo.o_parts = take((size_t)nparts * XB);
+    lo.o_parts_s = take((size_t)nparts * XB);
+    lo.o_wres = take((size_t)wins.size() * XB);
     lo.o_long = take((size_t)(1 + p.long_cap) * 4);
-    lo.o_carry = take((size_t)p.M * 128);
-    lo.o_results = take((size_t)p.M * 64);
+    lo.o_carry = take((size_t)p.M * XB);
+    lo.o_results = take((size_t)p.M * PB);
     lo.bytes = off;
     return true;
 }
@@ -352,15 +382,18 @@ static PlanPtrs plan_ptrs(const PlanLayout &L, size_t desc_off, size_t win_off, 
 // k_coarse_scatter (kernel 0) and k_seg_scatter (kernel 1) stage entries in
 // up to ~200 KB of shared memory: raise their dynamic shared-memory limit
 // once per device.
-static cudaError_t sort_smem(int device, int kernel, size_t bytes) {
+static cudaError_t sort_smem(int device, u32 curve, int kernel, size_t bytes) {
     static std::mutex mu;
     static std::map<std::pair<int, int>, size_t> done;
     std::lock_guard<std::mutex> g(mu);
-    size_t &have = done[std::make_pair(device, kernel)];
+    size_t &have = done[std::make_pair(device, kernel * 2 + (int)curve)];
     if (have >= bytes) return cudaSuccess;
-    cudaError_t e = kernel == 0
-                        ? cudaFuncSetAttribute(k_coarse_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes)
-                        : cudaFuncSetAttribute(k_seg_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    const int b = (int)bytes;
+    cudaError_t e;
+    if (kernel == 1) e = cudaFuncSetAttribute(k_seg_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    else if (curve == CURVE_BLS12381)
+        e = cudaFuncSetAttribute(k_coarse_scatter<Bls12381>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    else e = cudaFuncSetAttribute(k_coarse_scatter<Bn254>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e == cudaSuccess) have = bytes;
     return e;
 }
@@ -403,7 +436,7 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
         k_zero_words<<<1, 256, 0, st>>>(cnt + ncnt, cnt_pad - ncnt, p.longl, 1);
         CK_LAUNCH("k_zero_words");
         MARK(1);
-        k_coarse_count<<<sort_tiles, SORT_BLOCK, nbins * 4, st>>>(sa);
+        CURVE_LAUNCH(curve, k_coarse_count, sort_tiles, SORT_BLOCK, nbins * 4, st, sa);
         CK_LAUNCH("k_coarse_count");
         MARK(2);
         k_scan_reduce<<<cscan_tiles, SCAN_BLOCK, 0, st>>>(cnt, ctiles);
@@ -414,8 +447,8 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
         CK_LAUNCH("k_scan_down");
         MARK(3);
         const size_t scatter_smem = ((size_t)2 * nbins + 2 * STAGE_ENTRIES) * 4;
-        CK(sort_smem(device, 0, scatter_smem));
-        k_coarse_scatter<<<sort_tiles, SORT_BLOCK, scatter_smem, st>>>(sa);
+        CK(sort_smem(device, curve, 0, scatter_smem));
+        CURVE_LAUNCH(curve, k_coarse_scatter, sort_tiles, SORT_BLOCK, scatter_smem, st, sa);
         CK_LAUNCH("k_coarse_scatter");
         k_seg_plan<<<1, FINE_BLOCK, 0, st>>>(sa);
         CK_LAUNCH("k_seg_plan");
@@ -424,7 +457,7 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
         k_bin_scan<<<nbins, FINE_BLOCK, 0, st>>>(sa);
         CK_LAUNCH("k_bin_scan");
         const size_t seg_smem = (size_t)2 * FINE * 4 + (size_t)SEG_ENTRIES * 6;
-        CK(sort_smem(device, 1, seg_smem));
+        CK(sort_smem(device, curve, 1, seg_smem));
         k_seg_scatter<<<segcap, FINE_BLOCK, seg_smem, st>>>(sa);
         CK_LAUNCH("k_seg_scatter");
         MARK(4);
@@ -436,7 +469,7 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
         MARK(1);
 
         dim3 hgrid(hist_grid_x, M);
-        k_histogram<<<hgrid, 256, 0, st>>>(p.desc, p.counts);
+        CURVE_LAUNCH(curve, k_histogram, hgrid, 256, 0, st, p.desc, p.counts);
         CK_LAUNCH("k_histogram");
         MARK(2);
         k_scan_reduce<<<ntiles, SCAN_BLOCK, 0, st>>>(p.counts, p.tiles);
@@ -446,21 +479,21 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
         k_scan_down<<<ntiles, SCAN_BLOCK, 0, st>>>(p.counts, p.tiles, p.offsets, p.cursor, nb, ntiles);
         CK_LAUNCH("k_scan_down");
         MARK(3);
-        k_scatter<<<hgrid, 256, 0, st>>>(p.desc, p.cursor, p.entries);
+        CURVE_LAUNCH(curve, k_scatter, hgrid, 256, 0, st, p.desc, p.cursor, p.entries);
         CK_LAUNCH("k_scatter");
         MARK(4);
     }
 
     AccumArgs aa{p.entries, p.offsets, nb, points, p.buckets, p.recb, p.recp};
-    k_accumulate<<<accum_blocks, accum_block, 0, st>>>(aa);
+    CURVE_LAUNCH(curve, k_accumulate, accum_blocks, accum_block, 0, st, aa);
     CK_LAUNCH("k_accumulate");
     MARK(5);
 
     const u32 T = accum_blocks * accum_block;
     FixupArgs fa{p.offsets, nb, T, p.recb, p.recp, p.buckets, p.longl, long_cap};
-    k_fixup_short<<<(T + 255) / 256, 256, 0, st>>>(fa);
+    CURVE_LAUNCH(curve, k_fixup_short, (T + 255) / 256, 256, 0, st, fa);
     CK_LAUNCH("k_fixup_short");
-    k_fixup_long<<<(u32)sm_count(device), 256, 0, st>>>(fa);
+    CURVE_LAUNCH(curve, k_fixup_long, (u32)sm_count(device), 256, 0, st, fa);
     CK_LAUNCH("k_fixup_long");
     MARK(6);
     return cudaSuccess;
@@ -473,15 +506,15 @@ cudaError_t Plan::run_tail(void *scratch, const u32 *buckets, bool dense, u32 *r
     const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, tf_off, scratch, carry_ext, results, d_image);
     cudaError_t pe;
     ReduceArgs ra{p.wins, p.blk, p.offsets, buckets, p.parts, p.parts_s, dense ? 1u : 0u};
-    k_reduce<<<nrblocks, REDUCE_BLOCK, 0, st>>>(ra);
+    CURVE_LAUNCH(curve, k_reduce, nrblocks, REDUCE_BLOCK, 0, st, ra);
     CK_LAUNCH("k_reduce");
     MARK(7);
 
     WindowSumArgs wa{p.desc, p.wins, p.parts, p.parts_s, nwins, p.wres};
-    k_window_sum<<<nwins, WSUM_BLOCK, 0, st>>>(wa);
+    CURVE_LAUNCH(curve, k_window_sum, nwins, WSUM_BLOCK, 0, st, wa);
     CK_LAUNCH("k_window_sum");
     FinalArgs fa2{p.desc, p.wres, M, carry_mode == 0 ? nullptr : p.carry, carry_mode == 2 ? 0 : 1, p.res};
-    k_final<<<(M + 31) / 32, 32, 0, st>>>(fa2);
+    CURVE_LAUNCH(curve, k_final, (M + 31) / 32, 32, 0, st, fa2);
     CK_LAUNCH("k_final");
     MARK(8);
     return cudaSuccess;
@@ -510,7 +543,7 @@ cudaError_t Plan::launch_chunk(void *scratch, const u32 *points, u32 *acc, bool 
     if (e != cudaSuccess) return e;
     const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, tf_off, scratch, nullptr, nullptr, d_image);
     const u32 blocks = std::max(1u, std::min((nb + 255) / 256, (u32)sm_count(device) * 8));
-    k_bucket_merge<<<blocks, 256, 0, st>>>(p.offsets, p.buckets, acc, nb, first ? 1u : 0u);
+    CURVE_LAUNCH(curve, k_bucket_merge, blocks, 256, 0, st, p.offsets, p.buckets, acc, nb, first ? 1u : 0u);
     CK_LAUNCH("k_bucket_merge");
     return cudaSuccess;
 }
@@ -535,25 +568,27 @@ u32 *Plan::results_ptr(void *scratch) const {
     return reinterpret_cast<u32 *>(static_cast<unsigned char *>(scratch) + layout.o_results);
 }
 
-cudaError_t combine_xyzz(const u32 *d_xyzz, u32 k, u32 *d_out, cudaStream_t stream) {
-    k_combine<<<1, 32, 0, stream>>>(d_xyzz, k, d_out);
+cudaError_t combine_xyzz(const u32 *d_xyzz, u32 k, u32 *d_out, cudaStream_t stream, u32 curve) {
+    CURVE_LAUNCH(curve, k_combine, 1, 32, 0, stream, d_xyzz, k, d_out);
     CK_LAUNCH("k_combine");
     return cudaSuccess;
 }
 
+template <class C>
 __global__ void k_precompute(u32 *points, u64 n, u32 shift, u32 n_tables) {
+    using FQ = typename C::Fq;
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    Xyzz p = xyzz_from_affine(affine_load(points + i * 16));
+    XyzzT<FQ> p = xyzz_from_affine(affine_load<FQ>(points + i * C::PW));
     for (u32 j = 1; j < n_tables; j++) {
         for (u32 k = 0; k < shift; k++) p = xyzz_dbl(p);
-        affine_store(points + ((u64)j * n + i) * 16, xyzz_to_affine(p));
+        affine_store(points + ((u64)j * n + i) * C::PW, xyzz_to_affine(p));
     }
 }
 
-cudaError_t precompute_tables(u32 *d_points, u64 n, u32 shift, u32 n_tables, cudaStream_t stream) {
+cudaError_t precompute_tables(u32 *d_points, u64 n, u32 shift, u32 n_tables, cudaStream_t stream, u32 curve) {
     if (n == 0 || n_tables <= 1) return cudaSuccess;
-    k_precompute<<<(u32)((n + 127) / 128), 128, 0, stream>>>(d_points, n, shift, n_tables);
+    CURVE_LAUNCH(curve, k_precompute, (u32)((n + 127) / 128), 128, 0, stream, d_points, n, shift, n_tables);
     CK_LAUNCH("k_precompute");
     return cudaSuccess;
 }
@@ -662,8 +697,8 @@ static cudaError_t ctx_reserve(impeller_ctx *ctx, size_t bytes, cudaStream_t st)
 // table set for c every digit window shares one bucket set.
 MsmShape impeller::ctx_shape(const impeller_ctx *ctx, u32 n, u32 c) {
     const u32 base = ctx_set_base(ctx, c);
-    if (base != NONE) return MsmShape{n, c, 1, (u32)ctx->len, base};
-    return MsmShape{n, c, 0, 0, 0};
+    if (base != NONE) return MsmShape{n, c, 1, (u32)ctx->len, base, ctx->curve};
+    return MsmShape{n, c, 0, 0, 0, ctx->curve};
 }
 
 const u32 *impeller::ctx_point_base(const impeller_ctx *ctx) { return ctx->tables ? ctx->tables : ctx->points; }
@@ -708,16 +743,27 @@ cudaError_t impeller_set_window_table(const uint32_t *log2n, const uint32_t *c, 
 
 cudaError_t impeller_ctx_create(impeller_ctx **out, int device, const uint32_t *points, uint64_t len,
                                 int points_on_device) {
+    return impeller_ctx_create_curve(out, device, points, len, points_on_device, CURVE_BN254);
+}
+
+cudaError_t impeller_ctx_create_curve(impeller_ctx **out, int device, const uint32_t *points, uint64_t len,
+                                      int points_on_device, unsigned int curve) {
     if (!out || (!points && len)) {
         set_error("impeller_ctx_create: null argument");
         return cudaErrorInvalidValue;
     }
+    if (curve != CURVE_BN254 && curve != CURVE_BLS12381) {
+        set_error("impeller_ctx_create: unknown curve");
+        return cudaErrorInvalidValue;
+    }
+    const u64 PB = (u64)point_words(curve) * 4;
     if (len >= (1ull << 31)) {
         set_error("impeller_ctx_create: at most 2^31 - 1 points");
         return cudaErrorInvalidValue;
     }
     std::unique_ptr<impeller_ctx> ctx(new impeller_ctx());
     ctx->device = device;
+    ctx->curve = curve;
     ctx->len = len;
     CK(cudaSetDevice(device));
     CK(cudaEventCreateWithFlags(&ctx->done, cudaEventDisableTiming));
@@ -725,8 +771,8 @@ cudaError_t impeller_ctx_create(impeller_ctx **out, int device, const uint32_t *
         ctx->points = points;
     } else {
         u32 *d = nullptr;
-        CK(cudaMalloc(&d, std::max<u64>(len, 1) * 64));
-        cudaError_t e = cudaMemcpy(d, points, len * 64, cudaMemcpyHostToDevice);
+        CK(cudaMalloc(&d, std::max<u64>(len, 1) * PB));
+        cudaError_t e = cudaMemcpy(d, points, len * PB, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) {
             cudaFree(d);
             set_error(std::string("impeller_ctx_create: upload failed: ") + cudaGetErrorString(e));
@@ -735,7 +781,7 @@ cudaError_t impeller_ctx_create(impeller_ctx **out, int device, const uint32_t *
         ctx->points = d;
         ctx->owns = true;
     }
-    CK(cudaMalloc(&ctx->d_result, 64));
+    CK(cudaMalloc(&ctx->d_result, PB));
     *out = ctx.release();
     return cudaSuccess;
 }
@@ -766,7 +812,8 @@ cudaError_t impeller_ctx_precompute(impeller_ctx *ctx, unsigned int c) {
     if (ctx_set_base(ctx, c) != NONE) return cudaSuccess;
     CK(cudaSetDevice(ctx->device));
     CK(cudaDeviceSynchronize());
-    const u32 W = digit_windows(c);
+    const u32 W = digit_windows(c, ctx->curve);
+    const u64 PB = (u64)point_words(ctx->curve) * 4, PW = point_words(ctx->curve);
     const u64 have = ctx->tables ? ctx->tables_points : ctx->len;  // region 0 = the points
     const u64 total = have + (u64)W * ctx->len;
     if (total >= (1ull << 31)) {
@@ -774,12 +821,12 @@ cudaError_t impeller_ctx_precompute(impeller_ctx *ctx, unsigned int c) {
         return cudaErrorInvalidValue;
     }
     u32 *t = nullptr;
-    CK(cudaMalloc(&t, (size_t)std::max<u64>(total, 1) * 64));
+    CK(cudaMalloc(&t, (size_t)std::max<u64>(total, 1) * PB));
     const u32 *src = ctx->tables ? ctx->tables : ctx->points;
-    cudaError_t e = cudaMemcpy(t, src, have * 64, cudaMemcpyDeviceToDevice);
-    u32 *set = t + (size_t)have * 16;
-    if (e == cudaSuccess) e = cudaMemcpy(set, ctx->points, ctx->len * 64, cudaMemcpyDeviceToDevice);
-    if (e == cudaSuccess) e = precompute_tables(set, ctx->len, c, W, 0);
+    cudaError_t e = cudaMemcpy(t, src, have * PB, cudaMemcpyDeviceToDevice);
+    u32 *set = t + (size_t)have * PW;
+    if (e == cudaSuccess) e = cudaMemcpy(set, ctx->points, ctx->len * PB, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = precompute_tables(set, ctx->len, c, W, 0, ctx->curve);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         cudaFree(t);
@@ -803,7 +850,7 @@ static cudaError_t ctx_run_locked(impeller_ctx *ctx, const uint32_t *d_scalars, 
         set_error("MSM larger than the resident point array");
         return cudaErrorInvalidValue;
     }
-    if (n == 0) return cudaMemsetAsync(d_result, 0, 64, stream);
+    if (n == 0) return cudaMemsetAsync(d_result, 0, (size_t)point_words(ctx->curve) * 4, stream);
     if (c == 0) c = ctx_window(ctx, n);
     CK(cudaSetDevice(ctx->device));
     Plan *p = ctx_plan(ctx, (u32)n, c);
@@ -850,7 +897,8 @@ cudaError_t impeller_msm_host(impeller_ctx *ctx, const uint32_t *h_scalars, uint
     if (n) CK(cudaMemcpyAsync(ctx->d_scalars, h_scalars, n * 32, cudaMemcpyHostToDevice, stream));
     cudaError_t e = ctx_run_locked(ctx, ctx->d_scalars, n, c, ctx->d_result, stream);
     if (e != cudaSuccess) return e;
-    CK(cudaMemcpyAsync(h_result, ctx->d_result, 64, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(h_result, ctx->d_result, (size_t)point_words(ctx->curve) * 4, cudaMemcpyDeviceToHost,
+                       stream));
     CK(cudaStreamSynchronize(stream));
     return cudaSuccess;
 }
@@ -986,7 +1034,8 @@ cudaError_t impeller_batch_run(impeller_batch *b, const uint32_t *const *d_scala
         e = b->plan.mark_staged(stream);
         if (e != cudaSuccess) return e;
     }
-    CK(cudaMemcpyAsync(d_results, b->plan.results_ptr(b->scratch), (size_t)b->plan.M * 64, cudaMemcpyDeviceToDevice,
+    CK(cudaMemcpyAsync(d_results, b->plan.results_ptr(b->scratch), (size_t)b->plan.M * point_words(b->plan.curve) * 4,
+                       cudaMemcpyDeviceToDevice,
                        stream));
     return cudaSuccess;
 }

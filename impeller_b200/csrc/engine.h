@@ -20,16 +20,28 @@ typedef uint64_t u64;
 void set_error(const std::string &msg);
 const char *last_error();
 
-// Shape of one MSM in a plan.
+// Curves (the reference's MSM_CURVE values bn254 and bls12381).
+enum : u32 { CURVE_BN254 = 0, CURVE_BLS12381 = 1 };
+
+// Affine point and XYZZ point size in 32-bit words, per curve.
+inline u32 point_words(u32 curve) { return curve == CURVE_BLS12381 ? 24u : 16u; }
+inline u32 xyzz_words(u32 curve) { return curve == CURVE_BLS12381 ? 48u : 32u; }
+
+// Shape of one MSM in a plan (every MSM of a plan is on the same curve).
 struct MsmShape {
     u32 n;             // points / scalars
     u32 c;             // window bits
     u32 n_windows;     // bucket sets (physical windows); 0 -> one per digit window
     u32 table_stride;  // points per window table (used when n_windows < digit windows)
     u32 table_base;    // point index of this MSM's table 0
+    u32 curve;         // CURVE_BN254 or CURVE_BLS12381
 };
 
-u32 digit_windows(u32 c);  // ceil(254 / c)
+// Signed-digit windows of width c for the curve's scalars: the fewest that
+// keep the top digit plus its incoming carry at most 2^(c-1).  BN254
+// (r < 2^254): ceil(254 / c); BLS12-381 (r < 2^255): ceil(255 / c) or one
+// more (c = 3, 5, 15, 17).
+u32 digit_windows(u32 c, u32 curve = CURVE_BN254);
 u32 default_window(u64 n);  // autotune table (or the cost model)
 u32 table_window(u64 n);    // tables window the autotune table recommends (0: none)
 
@@ -90,7 +102,7 @@ class Plan {
                              const void *d_image = nullptr);
     cudaError_t launch_chunked_tail(void *scratch, const u32 *acc, u32 *results, int carry_mode,
                                     cudaStream_t stream, u32 *carry_ext = nullptr, const void *d_image = nullptr);
-    size_t acc_bytes() const { return (size_t)nb * 128; }
+    size_t acc_bytes() const { return (size_t)nb * xyzz_words(curve) * 4; }
     // The table image (descriptors with these scalar pointers, windows,
     // reduce blocks) as launch uploads it, written to host memory at dst.
     size_t image_bytes() const;
@@ -102,6 +114,7 @@ class Plan {
     u32 *results_ptr(void *scratch) const;
 
     int device = 0;
+    u32 curve = CURVE_BN254;
     u32 M = 0;
     u32 nb = 0, nb_pad = 0, ntiles = 0;
     u64 max_entries = 0;
@@ -145,16 +158,18 @@ class Plan {
 };
 
 // k_combine: sum `k` XYZZ points in device memory, write canonical affine.
-cudaError_t combine_xyzz(const u32 *d_xyzz, u32 k, u32 *d_out, cudaStream_t stream);
+cudaError_t combine_xyzz(const u32 *d_xyzz, u32 k, u32 *d_out, cudaStream_t stream, u32 curve = CURVE_BN254);
 
 // Window tables 2^(j*shift)*P for j in 1..n_tables-1, in place after table 0.
-cudaError_t precompute_tables(u32 *d_points, u64 n, u32 shift, u32 n_tables, cudaStream_t stream);
+cudaError_t precompute_tables(u32 *d_points, u64 n, u32 shift, u32 n_tables, cudaStream_t stream,
+                              u32 curve = CURVE_BN254);
 
 }  // namespace impeller
 
 // Resident-SRS context (the C ABI's opaque impeller_ctx).
 struct impeller_ctx {
     int device = 0;
+    impeller::u32 curve = impeller::CURVE_BN254;
     const impeller::u32 *points = nullptr;
     impeller::u64 len = 0;
     bool owns = false;

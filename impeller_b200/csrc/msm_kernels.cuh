@@ -32,7 +32,7 @@
 
 namespace impeller {
 
-using namespace bn254;
+using namespace ec;
 
 static constexpr u32 NONE = 0xffffffffu;
 static constexpr u32 SCAN_BLOCK = 256;
@@ -72,8 +72,9 @@ struct WinDesc {
 // the top digit plus an incoming carry at most 2^(c-1), a valid bucket.
 // Windows are taken in order, w = 0, 1, ...: the scalar is shifted right by
 // c after each window, so the next digit is always the low c bits of limb 0.
+template <class FR>
 struct DigitIter {
-    Fr v;
+    Fe<FR> v;
     u32 c, carry;
     __device__ __forceinline__ void next(u32 w, u32 n_logical, u32 &mag, u32 &sign) {
         const u32 raw = v.l[0] & ((1u << c) - 1u);
@@ -100,6 +101,7 @@ struct DigitIter {
 // witness-like inputs) would otherwise serialize on a handful of addresses.
 // Every lane of the warp runs the same number of windows, so the match is
 // always taken with the full warp present.
+template <class C>
 __global__ void k_histogram(const MsmDesc *__restrict__ descs, u32 *__restrict__ counts) {
     const MsmDesc d = descs[blockIdx.y];
     const u32 B = 1u << (d.c - 1);
@@ -108,8 +110,9 @@ __global__ void k_histogram(const MsmDesc *__restrict__ descs, u32 *__restrict__
     for (u32 base = blockIdx.x * blockDim.x; base < d.n; base += stride) {
         const u32 i = base + threadIdx.x;
         const bool live = i < d.n;
-        DigitIter it;
-        it.v = live ? fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i)) : fe_zero<FrP>();
+        DigitIter<typename C::Fr> it;
+        it.v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
+                    : fe_zero<typename C::Fr>();
         it.c = d.c;
         it.carry = 0;
         for (u32 w = 0; w < d.n_logical; w++) {
@@ -122,6 +125,7 @@ __global__ void k_histogram(const MsmDesc *__restrict__ descs, u32 *__restrict__
     }
 }
 
+template <class C>
 __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ cursor, u32 *__restrict__ entries) {
     const MsmDesc d = descs[blockIdx.y];
     const u32 B = 1u << (d.c - 1);
@@ -130,8 +134,9 @@ __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ c
     for (u32 base = blockIdx.x * blockDim.x; base < d.n; base += stride) {
         const u32 i = base + threadIdx.x;
         const bool live = i < d.n;
-        DigitIter it;
-        it.v = live ? fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i)) : fe_zero<FrP>();
+        DigitIter<typename C::Fr> it;
+        it.v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
+                    : fe_zero<typename C::Fr>();
         it.c = d.c;
         it.carry = 0;
         for (u32 w = 0; w < d.n_logical; w++) {
@@ -243,6 +248,7 @@ __device__ __forceinline__ void sort_tile(const SortArgs &a, u32 tile, u32 &m, u
     end = min(start + a.tile_scalars, a.descs[m].n);
 }
 
+template <class C>
 __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
     extern __shared__ u32 hist[];  // nbins
     u32 m, start, end;
@@ -254,8 +260,9 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
     for (u32 base = start; base < end; base += blockDim.x) {
         const u32 i = base + threadIdx.x;
         const bool live = i < end;
-        DigitIter it;
-        it.v = live ? fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i)) : fe_zero<FrP>();
+        DigitIter<typename C::Fr> it;
+        it.v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
+                    : fe_zero<typename C::Fr>();
         it.c = d.c;
         it.carry = 0;
         for (u32 w = 0; w < d.n_logical; w++) {
@@ -271,6 +278,7 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
 // Shared memory: delta[nbins], cur[nbins], stage_e[STAGE_ENTRIES],
 // stage_f[STAGE_ENTRIES].  A tile holds at most STAGE_ENTRIES entries (the
 // plan sizes tiles by the largest window count).
+template <class C>
 __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_scatter(SortArgs a) {
     extern __shared__ u32 sm[];
     __shared__ u32 warp_tot[32];
@@ -302,8 +310,9 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_scatter(SortArgs a) {
     for (u32 base = start; base < end; base += blockDim.x) {
         const u32 i = base + threadIdx.x;
         const bool live = i < end;
-        DigitIter it;
-        it.v = live ? fe_from_mont<FrP>(fe_load<FrP>(d.scalars + 8ull * i)) : fe_zero<FrP>();
+        DigitIter<typename C::Fr> it;
+        it.v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
+                    : fe_zero<typename C::Fr>();
         it.c = d.c;
         it.carry = 0;
         for (u32 w = 0; w < d.n_logical; w++) {
@@ -521,9 +530,10 @@ struct AccumArgs {
     u32 *rec_point;      // 2 per thread, XYZZ
 };
 
-__device__ __forceinline__ Affine load_entry_point(const u32 *__restrict__ points, u32 e) {
-    Affine q = affine_load(points + (size_t)(e >> 1) * 16);
-    if (e & 1u) q.y = fe_neg<FqP>(q.y);
+template <class C>
+__device__ __forceinline__ AffineT<typename C::Fq> load_entry_point(const u32 *__restrict__ points, u32 e) {
+    AffineT<typename C::Fq> q = affine_load<typename C::Fq>(points + (size_t)(e >> 1) * C::PW);
+    if (e & 1u) q.y = fe_neg(q.y);
     return q;
 }
 
@@ -545,7 +555,9 @@ __device__ __forceinline__ Affine load_entry_point(const u32 *__restrict__ point
 static constexpr u32 ACCUM_BLOCK = ACCUM_THREADS;
 static constexpr u32 ACCUM_PER_SM = ACCUM_BLOCKS_PER_SM;
 
+template <class C>
 __global__ void __launch_bounds__(ACCUM_THREADS, ACCUM_BLOCKS_PER_SM) k_accumulate(AccumArgs a) {
+    using FQ = typename C::Fq;
     const u32 T = gridDim.x * blockDim.x;
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 E = a.offsets[a.nb];
@@ -568,12 +580,12 @@ __global__ void __launch_bounds__(ACCUM_THREADS, ACCUM_BLOCKS_PER_SM) k_accumula
     u32 bbeg = a.offsets[b], bend = a.offsets[b + 1];
     u32 seg_end = min(bend, end);
 
-    Xyzz acc = xyzz_identity();
+    XyzzT<FQ> acc = xyzz_identity<FQ>();
     bool fresh = true;
-    Affine nxt = load_entry_point(a.points, a.entries[start]);
+    AffineT<FQ> nxt = load_entry_point<C>(a.points, a.entries[start]);
     for (u32 pos = start; pos < end; pos++) {
-        Affine q = nxt;
-        if (pos + 1 < end) nxt = load_entry_point(a.points, a.entries[pos + 1]);
+        AffineT<FQ> q = nxt;
+        if (pos + 1 < end) nxt = load_entry_point<C>(a.points, a.entries[pos + 1]);
         if (fresh) {
             acc = xyzz_from_affine(q);
             fresh = false;
@@ -582,11 +594,11 @@ __global__ void __launch_bounds__(ACCUM_THREADS, ACCUM_BLOCKS_PER_SM) k_accumula
         }
         if (pos + 1 == seg_end) {
             if (bbeg >= start && bend <= end) {
-                xyzz_store(a.buckets + (size_t)b * 32, acc);
+                xyzz_store(a.buckets + (size_t)b * C::XW, acc);
             } else {
                 u32 slot = bbeg < start ? 2 * t : 2 * t + 1;
                 a.rec_bucket[slot] = b;
-                xyzz_store(a.rec_point + (size_t)slot * 32, acc);
+                xyzz_store(a.rec_point + (size_t)slot * C::XW, acc);
             }
             fresh = true;
             if (pos + 1 < end) {
@@ -614,7 +626,9 @@ struct FixupArgs {
 
 // Owner of a cut bucket = the slice where the bucket begins (record 2t+1).
 // The bucket continues as the first piece (record 2t') of slices t+1 .. t1.
+template <class C>
 __global__ void k_fixup_short(FixupArgs f) {
+    using FQ = typename C::Fq;
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= f.T) return;
     const u32 b = f.rec_bucket[2 * t + 1];
@@ -627,13 +641,15 @@ __global__ void k_fixup_short(FixupArgs f) {
         if (k < f.long_cap) f.long_list[1 + k] = t;
         return;
     }
-    Xyzz acc = xyzz_load(f.rec_point + (size_t)(2 * t + 1) * 32);
-    for (u32 s = t + 1; s <= t1; s++) acc = xyzz_add(acc, xyzz_load(f.rec_point + (size_t)(2 * s) * 32));
-    xyzz_store(f.buckets + (size_t)b * 32, acc);
+    XyzzT<FQ> acc = xyzz_load<FQ>(f.rec_point + (size_t)(2 * t + 1) * C::XW);
+    for (u32 s = t + 1; s <= t1; s++) acc = xyzz_add(acc, xyzz_load<FQ>(f.rec_point + (size_t)(2 * s) * C::XW));
+    xyzz_store(f.buckets + (size_t)b * C::XW, acc);
 }
 
 // One warp per long run (a bucket spread over more than 5 slices).
+template <class C>
 __global__ void k_fixup_long(FixupArgs f) {
+    using FQ = typename C::Fq;
     const u32 lane = threadIdx.x & 31u;
     const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
     const u32 count = min(f.long_list[0], f.long_cap);
@@ -643,12 +659,13 @@ __global__ void k_fixup_long(FixupArgs f) {
         const u32 t = f.long_list[1 + w];
         const u32 b = f.rec_bucket[2 * t + 1];
         const u32 t1 = (f.offsets[b + 1] - 1) / L;
-        Xyzz acc = xyzz_identity();
-        if (lane == 0) acc = xyzz_load(f.rec_point + (size_t)(2 * t + 1) * 32);
-        for (u32 s = t + 1 + lane; s <= t1; s += 32) acc = xyzz_add(acc, xyzz_load(f.rec_point + (size_t)(2 * s) * 32));
+        XyzzT<FQ> acc = xyzz_identity<FQ>();
+        if (lane == 0) acc = xyzz_load<FQ>(f.rec_point + (size_t)(2 * t + 1) * C::XW);
+        for (u32 s = t + 1 + lane; s <= t1; s += 32)
+            acc = xyzz_add(acc, xyzz_load<FQ>(f.rec_point + (size_t)(2 * s) * C::XW));
 #pragma unroll 1
         for (u32 o = 16; o; o >>= 1) acc = xyzz_add(acc, xyzz_shfl_down(acc, o));
-        if (lane == 0) xyzz_store(f.buckets + (size_t)b * 32, acc);
+        if (lane == 0) xyzz_store(f.buckets + (size_t)b * C::XW, acc);
     }
 }
 
@@ -656,15 +673,18 @@ __global__ void k_fixup_long(FixupArgs f) {
 // sort and the accumulation per chunk and adds each chunk's bucket sums into
 // persistent accumulators `acc` (nb XYZZ); the reduction runs once, over
 // `acc` (dense).  first: acc = this chunk's sums (identity where empty).
+template <class C>
 __global__ void k_bucket_merge(const u32 *__restrict__ offsets, const u32 *__restrict__ buckets,
                                u32 *__restrict__ acc, u32 nb, u32 first) {
+    using FQ = typename C::Fq;
+    constexpr u32 XW = C::XW;
     for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
         const bool filled = offsets[g + 1] != offsets[g];
         if (first) {
-            xyzz_store(acc + (size_t)g * 32, filled ? xyzz_load(buckets + (size_t)g * 32) : xyzz_identity());
+            xyzz_store(acc + (size_t)g * XW, filled ? xyzz_load<FQ>(buckets + (size_t)g * XW) : xyzz_identity<FQ>());
         } else if (filled) {
-            xyzz_store(acc + (size_t)g * 32,
-                       xyzz_add(xyzz_load(acc + (size_t)g * 32), xyzz_load(buckets + (size_t)g * 32)));
+            xyzz_store(acc + (size_t)g * XW,
+                       xyzz_add(xyzz_load<FQ>(acc + (size_t)g * XW), xyzz_load<FQ>(buckets + (size_t)g * XW)));
         }
     }
 }
@@ -697,36 +717,40 @@ static constexpr u32 REDUCE_WARPS = REDUCE_BLOCK / 32;
 
 __device__ __forceinline__ u32 ilog2(u32 x) { return 31 - __clz(x); }
 
+template <class C>
 __global__ void __launch_bounds__(REDUCE_BLOCK, 3) k_reduce(ReduceArgs r) {
+    using FQ = typename C::Fq;
+    using Xz = XyzzT<FQ>;
     const uint2 blk = r.blocks[blockIdx.x];
     const WinDesc wd = r.wins[blk.x];
     const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     const u32 j = blk.y * REDUCE_BLOCK + threadIdx.x;
     const u32 lo = j * wd.chunk;  // weights lo+1 .. lo+chunk
-    Xyzz sum = xyzz_identity(), sos = xyzz_identity();
+    Xz sum = xyzz_identity<FQ>(), sos = xyzz_identity<FQ>();
     if (lo < wd.nbuckets) {
         const u32 hi = min(lo + wd.chunk, wd.nbuckets);
         for (u32 k = hi; k > lo; k--) {
             const u32 g = wd.bucket_base + k - 1;
-            if (r.dense || r.offsets[g + 1] != r.offsets[g]) sum = xyzz_add(sum, xyzz_load(r.buckets + (size_t)g * 32));
+            if (r.dense || r.offsets[g + 1] != r.offsets[g])
+                sum = xyzz_add(sum, xyzz_load<FQ>(r.buckets + (size_t)g * C::XW));
             sos = xyzz_add(sos, sum);
         }
     }
     // inclusive suffix of `sum` inside the warp
-    Xyzz x = sum;
+    Xz x = sum;
 #pragma unroll 1
     for (u32 o = 1; o < 32; o <<= 1) {
-        Xyzz y = xyzz_shfl_down(x, o);
+        Xz y = xyzz_shfl_down(x, o);
         if (lane + o < 32) x = xyzz_add(x, y);
     }
-    Xyzz ex = xyzz_shfl_down(x, 1);
-    if (lane == 31) ex = xyzz_identity();
+    Xz ex = xyzz_shfl_down(x, 1);
+    if (lane == 31) ex = xyzz_identity<FQ>();
     for (u32 k = 0, lg = ilog2(wd.chunk); k < lg; k++) ex = xyzz_dbl(ex);
-    Xyzz v = xyzz_add(sos, ex);
+    Xz v = xyzz_add(sos, ex);
 #pragma unroll 1
     for (u32 o = 16; o; o >>= 1) v = xyzz_add(v, xyzz_shfl_down(v, o));
     if (lane == 0) {
-        const size_t slot = (size_t)(wd.part_base + blk.y * REDUCE_WARPS + wid) * 32;
+        const size_t slot = (size_t)(wd.part_base + blk.y * REDUCE_WARPS + wid) * C::XW;
         xyzz_store(r.parts_v + slot, v);
         xyzz_store(r.parts_s + slot, x);
     }
@@ -747,9 +771,12 @@ static constexpr u32 WSUM_WARPS = WSUM_BLOCK / 32;
 // One block per window: T = sum_w V_w + 32 L * sum_w w * S_w (thread t owns a
 // group of g consecutive warp partials, a block-wide suffix scan gives the
 // cross-group weights).  k_final weights the windows by 2^(c * window).
+template <class C>
 __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
-    __shared__ __align__(16) u32 sm_a[WSUM_WARPS][32];
-    __shared__ __align__(16) u32 sm_b[WSUM_WARPS][32];
+    using FQ = typename C::Fq;
+    using Xz = XyzzT<FQ>;
+    __shared__ __align__(16) u32 sm_a[WSUM_WARPS][C::XW];
+    __shared__ __align__(16) u32 sm_b[WSUM_WARPS][C::XW];
     const u32 win = blockIdx.x;
     if (win >= a.nwins) return;
     const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
@@ -759,38 +786,38 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
     const u32 b0 = threadIdx.x * g;
     const u32 top = min(b0 + g, wd.nparts);
     // group-local weights: partial b carries weight b - b0
-    Xyzz vsum = xyzz_identity(), ssum = xyzz_identity(), sos = xyzz_identity();
+    Xz vsum = xyzz_identity<FQ>(), ssum = xyzz_identity<FQ>(), sos = xyzz_identity<FQ>();
     for (u32 b = top; b > b0; b--) {
-        const size_t slot = (size_t)(wd.part_base + b - 1) * 32;
+        const size_t slot = (size_t)(wd.part_base + b - 1) * C::XW;
         if (b < top) sos = xyzz_add(sos, ssum);
-        vsum = xyzz_add(vsum, xyzz_load(a.parts_v + slot));
-        ssum = xyzz_add(ssum, xyzz_load(a.parts_s + slot));
+        vsum = xyzz_add(vsum, xyzz_load<FQ>(a.parts_v + slot));
+        ssum = xyzz_add(ssum, xyzz_load<FQ>(a.parts_s + slot));
     }
     // block-wide inclusive suffix of ssum: warp scan, then a scan of the warp totals
-    Xyzz x = ssum;
+    Xz x = ssum;
 #pragma unroll 1
     for (u32 o = 1; o < 32; o <<= 1) {
-        Xyzz y = xyzz_shfl_down(x, o);
+        Xz y = xyzz_shfl_down(x, o);
         if (lane + o < 32) x = xyzz_add(x, y);
     }
     if (lane == 0) xyzz_store(&sm_a[wid][0], x);
     __syncthreads();
     if (wid == 0) {
-        Xyzz t = lane < WSUM_WARPS ? xyzz_load(&sm_a[lane][0]) : xyzz_identity();
+        Xz t = lane < WSUM_WARPS ? xyzz_load<FQ>(&sm_a[lane][0]) : xyzz_identity<FQ>();
 #pragma unroll 1
         for (u32 o = 1; o < WSUM_WARPS; o <<= 1) {
-            Xyzz y = xyzz_shfl_down(t, o);
+            Xz y = xyzz_shfl_down(t, o);
             if (lane + o < WSUM_WARPS) t = xyzz_add(t, y);
         }
         if (lane < WSUM_WARPS) xyzz_store(&sm_b[lane][0], t);  // suffix over warps >= lane
     }
     __syncthreads();
-    Xyzz later = wid + 1 < WSUM_WARPS ? xyzz_load(&sm_b[wid + 1][0]) : xyzz_identity();
-    Xyzz ex = xyzz_shfl_down(x, 1);
-    if (lane == 31) ex = xyzz_identity();
+    Xz later = wid + 1 < WSUM_WARPS ? xyzz_load<FQ>(&sm_b[wid + 1][0]) : xyzz_identity<FQ>();
+    Xz ex = xyzz_shfl_down(x, 1);
+    if (lane == 31) ex = xyzz_identity<FQ>();
     ex = xyzz_add(ex, later);
     for (u32 k = 0, lg = ilog2(g); k < lg; k++) ex = xyzz_dbl(ex);
-    Xyzz rs = xyzz_add(sos, ex);  // this group's share of sum_w w * S_w
+    Xz rs = xyzz_add(sos, ex);  // this group's share of sum_w w * S_w
 #pragma unroll 1
     for (u32 o = 16; o; o >>= 1) {
         rs = xyzz_add(rs, xyzz_shfl_down(rs, o));
@@ -803,8 +830,8 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
     }
     __syncthreads();
     if (wid == 0) {
-        Xyzz r2 = lane < WSUM_WARPS ? xyzz_load(&sm_a[lane][0]) : xyzz_identity();
-        Xyzz v2 = lane < WSUM_WARPS ? xyzz_load(&sm_b[lane][0]) : xyzz_identity();
+        Xz r2 = lane < WSUM_WARPS ? xyzz_load<FQ>(&sm_a[lane][0]) : xyzz_identity<FQ>();
+        Xz v2 = lane < WSUM_WARPS ? xyzz_load<FQ>(&sm_b[lane][0]) : xyzz_identity<FQ>();
 #pragma unroll 1
         for (u32 o = WSUM_WARPS / 2; o; o >>= 1) {
             r2 = xyzz_add(r2, xyzz_shfl_down(r2, o));
@@ -813,7 +840,7 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
         if (lane == 0) {
             const u32 shift = ilog2(wd.chunk) + 5;  // 32 lanes per warp partial
             for (u32 k = 0; k < shift; k++) r2 = xyzz_dbl(r2);
-            xyzz_store(a.wres + (size_t)win * 32, xyzz_add(v2, r2));
+            xyzz_store(a.wres + (size_t)win * C::XW, xyzz_add(v2, r2));
         }
     }
 }
@@ -824,35 +851,38 @@ struct FinalArgs {
     u32 M;
     u32 *carry;       // optional XYZZ per MSM: added in, or written when !emit_affine
     int emit_affine;  // write canonical affine results
-    u32 *results;     // 16 u32 per MSM
+    u32 *results;     // one affine point (C::PW words) per MSM
 };
 
 // One thread per MSM: Horner over its windows, sum_w 2^(c w) T_w with
 // c * (windows - 1) doublings, then the carry and the affine form.
+template <class C>
 __global__ void k_final(FinalArgs f) {
+    using FQ = typename C::Fq;
     const u32 m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= f.M) return;
     const MsmDesc d = f.descs[m];
-    Xyzz acc = xyzz_identity();
+    XyzzT<FQ> acc = xyzz_identity<FQ>();
     for (int w = (int)d.n_windows - 1; w >= 0; w--) {
         if (!xyzz_is_identity(acc))
             for (u32 k = 0; k < d.c; k++) acc = xyzz_dbl(acc);
-        acc = xyzz_add(acc, xyzz_load(f.wres + (size_t)(d.win_base + w) * 32));
+        acc = xyzz_add(acc, xyzz_load<FQ>(f.wres + (size_t)(d.win_base + w) * C::XW));
     }
-    if (f.carry) acc = xyzz_add(acc, xyzz_load(f.carry + (size_t)m * 32));
+    if (f.carry) acc = xyzz_add(acc, xyzz_load<FQ>(f.carry + (size_t)m * C::XW));
     if (f.emit_affine) {
-        Affine r = xyzz_to_affine_fast(acc);
-        affine_store(f.results + (size_t)m * 16, r);
+        affine_store(f.results + (size_t)m * C::PW, xyzz_to_affine_fast(acc));
     } else {
-        xyzz_store(f.carry + (size_t)m * 32, acc);
+        xyzz_store(f.carry + (size_t)m * C::XW, acc);
     }
 }
 
 // Sum of k XYZZ points (per-card partials) to canonical affine.
+template <class C>
 __global__ void k_combine(const u32 *xyzz, u32 k, u32 *out) {
+    using FQ = typename C::Fq;
     if (blockIdx.x || threadIdx.x) return;
-    Xyzz acc = xyzz_identity();
-    for (u32 i = 0; i < k; i++) acc = xyzz_add(acc, xyzz_load(xyzz + (size_t)i * 32));
+    XyzzT<FQ> acc = xyzz_identity<FQ>();
+    for (u32 i = 0; i < k; i++) acc = xyzz_add(acc, xyzz_load<FQ>(xyzz + (size_t)i * C::XW));
     affine_store(out, xyzz_to_affine_fast(acc));
 }
 

@@ -199,7 +199,7 @@ extern "C" cudaError_t impeller_msm_device_noalloc(const uint32_t *d_points, con
     NA_LAUNCHED("k_noalloc_tables");
     NA_CK(cudaMemsetAsync(counts, 0, (size_t)NB_PAD * 4, stream));
     const dim3 hgrid((u32)((n + 255) / 256), 1);
-    K::k_histogram<<<hgrid, 256, 0, stream>>>(desc, counts);
+    K::k_histogram<K::Bn254><<<hgrid, 256, 0, stream>>>(desc, counts);
     NA_LAUNCHED("k_histogram");
     K::k_scan_reduce<<<NTILES, K::SCAN_BLOCK, 0, stream>>>(counts, tiles);
     NA_LAUNCHED("k_scan_reduce");
@@ -207,25 +207,25 @@ extern "C" cudaError_t impeller_msm_device_noalloc(const uint32_t *d_points, con
     NA_LAUNCHED("k_scan_tiles");
     K::k_scan_down<<<NTILES, K::SCAN_BLOCK, 0, stream>>>(counts, tiles, offsets, cursor, NB, NTILES);
     NA_LAUNCHED("k_scan_down");
-    K::k_scatter<<<hgrid, 256, 0, stream>>>(desc, cursor, entries);
+    K::k_scatter<K::Bn254><<<hgrid, 256, 0, stream>>>(desc, cursor, entries);
     NA_LAUNCHED("k_scatter");
     AccumArgs aa{entries, offsets, NB, d_points, buckets, recb, recp};
-    K::k_accumulate<<<ACC_BLOCKS, ACC_THREADS, 0, stream>>>(aa);
+    K::k_accumulate<K::Bn254><<<ACC_BLOCKS, ACC_THREADS, 0, stream>>>(aa);
     NA_LAUNCHED("k_accumulate");
     NA_CK(cudaMemsetAsync(longl, 0, 4, stream));
     FixupArgs fa{offsets, NB, T, recb, recp, buckets, longl, T};
-    K::k_fixup_short<<<T / 256, 256, 0, stream>>>(fa);
+    K::k_fixup_short<K::Bn254><<<T / 256, 256, 0, stream>>>(fa);
     NA_LAUNCHED("k_fixup_short");
-    K::k_fixup_long<<<64, 256, 0, stream>>>(fa);
+    K::k_fixup_long<K::Bn254><<<64, 256, 0, stream>>>(fa);
     NA_LAUNCHED("k_fixup_long");
     ReduceArgs ra{wins, rblk, offsets, buckets, parts_v, parts_s};
-    K::k_reduce<<<NRBLOCKS, K::REDUCE_BLOCK, 0, stream>>>(ra);
+    K::k_reduce<K::Bn254><<<NRBLOCKS, K::REDUCE_BLOCK, 0, stream>>>(ra);
     NA_LAUNCHED("k_reduce");
     WindowSumArgs wa{desc, wins, parts_v, parts_s, W, wres};
-    K::k_window_sum<<<W, K::WSUM_BLOCK, 0, stream>>>(wa);
+    K::k_window_sum<K::Bn254><<<W, K::WSUM_BLOCK, 0, stream>>>(wa);
     NA_LAUNCHED("k_window_sum");
     FinalArgs fin{desc, wres, 1, nullptr, 1, d_result};
-    K::k_final<<<1, 128, 0, stream>>>(fin);
+    K::k_final<K::Bn254><<<1, 128, 0, stream>>>(fin);
     NA_LAUNCHED("k_final");
     return cudaSuccess;
 }

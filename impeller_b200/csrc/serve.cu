@@ -51,7 +51,7 @@ struct Job {
     double t_submit = 0, t_done = 0;
     bool done = false;
     cudaError_t status = cudaSuccess;
-    u32 result[16] = {};
+    u32 result[24] = {};  // affine result, point_words(curve) used
 };
 
 struct Batch {
@@ -61,7 +61,7 @@ struct Batch {
     cudaEvent_t ev = nullptr;
     void *mem = nullptr;  // scalars | results | plan scratch
     size_t bytes = 0;
-    u32 *h_results = nullptr;  // pinned, 16 u32 per job
+    u32 *h_results = nullptr;  // pinned, point_words(curve) u32 per job
     cudaError_t status = cudaSuccess;
 };
 
@@ -106,7 +106,8 @@ cudaError_t launch_batch(impeller_server *s, Batch &b, std::vector<Job *> &js, u
     if (!Plan::build(*b.plan, s->ctx->device, shapes)) return cudaErrorInvalidValue;
     b.plan->set_staging(s->staging[slot], s->staging_cap);
     const size_t o_res = up256(scal_words * 4);
-    const size_t o_plan = o_res + up256((size_t)M * 64);
+    const size_t RB = (size_t)point_words(s->ctx->curve) * 4;  // result bytes per job
+    const size_t o_plan = o_res + up256((size_t)M * RB);
     b.bytes = o_plan + b.plan->scratch_bytes();
     b.stream = s->streams[slot];
     b.h_results = s->pinned[slot];
@@ -126,17 +127,18 @@ cudaError_t launch_batch(impeller_server *s, Batch &b, std::vector<Job *> &js, u
     u32 *d_res = reinterpret_cast<u32 *>(base + o_res);
     if ((e = b.plan->enqueue(base + o_plan, ctx_point_base(s->ctx), sc.data(), d_res, 0, b.stream)) != cudaSuccess)
         return e;
-    if ((e = cudaMemcpyAsync(b.h_results, d_res, (size_t)M * 64, cudaMemcpyDeviceToHost, b.stream)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(b.h_results, d_res, (size_t)M * RB, cudaMemcpyDeviceToHost, b.stream)) != cudaSuccess)
         return e;
     if ((e = cudaEventRecord(b.ev, b.stream)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
 void finish_batch(impeller_server *s, Batch &b, double t) {
+    const u32 PW = point_words(s->ctx->curve);
     for (size_t k = 0; k < b.ids.size(); k++) {
         Job &j = s->jobs[b.ids[k]];
         j.status = b.status;
-        if (b.status == cudaSuccess) std::memcpy(j.result, b.h_results + 16 * k, 64);
+        if (b.status == cudaSuccess) std::memcpy(j.result, b.h_results + PW * k, PW * 4);
         j.done = true;
         j.t_done = t;
         if (b.status == cudaSuccess) {
@@ -252,7 +254,9 @@ cudaError_t impeller_server_create(impeller_server **out, impeller_ctx *ctx, uin
         if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return e;
         s->streams.push_back(st);
         u32 *p = nullptr;
-        if ((e = cudaHostAlloc(&p, (size_t)max_batch * 64, cudaHostAllocPortable)) != cudaSuccess) return e;
+        if ((e = cudaHostAlloc(&p, (size_t)max_batch * point_words(ctx->curve) * 4, cudaHostAllocPortable)) !=
+            cudaSuccess)
+            return e;
         s->pinned.push_back(p);
         void *t = nullptr;
         s->staging_cap = (size_t)max_batch * 4096 + (1u << 20);  // descriptors, windows, reduce blocks
@@ -302,7 +306,7 @@ static cudaError_t take_result(impeller_server *s, std::unordered_map<u64, Job>:
                                double *latency_ms) {
     Job &j = it->second;
     cudaError_t st = j.status;
-    if (h_result && st == cudaSuccess) std::memcpy(h_result, j.result, 64);
+    if (h_result && st == cudaSuccess) std::memcpy(h_result, j.result, point_words(s->ctx->curve) * 4);
     if (latency_ms) *latency_ms = (j.t_done - j.t_submit) * 1e3;
     s->jobs.erase(it);
     if (st != cudaSuccess) set_error(std::string("MSM job failed: ") + cudaGetErrorString(st));

@@ -28,8 +28,17 @@ SIGNATURES: dict[str, tuple] = {
     "impeller_msm_precompute_cfg": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, ctypes.c_ulonglong, c_u32pp,
                                                    ctypes.c_uint]),
     "impeller_msm_n_precompute": (ctypes.c_uint, [ctypes.c_uint, ctypes.c_uint]),
+    "impeller_msm_cfg_curve": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_int, c_void_pp,
+                                              c_ulong_p, ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint,
+                                              ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, c_u32p, c_u32pp,
+                                              ctypes.c_uint, c_u32pp, c_u32pp]),
+    "impeller_msm_precompute_cfg_curve": (ctypes.c_int, [ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
+                                                         ctypes.c_ulonglong, c_u32pp, ctypes.c_uint]),
+    "impeller_msm_n_precompute_curve": (ctypes.c_uint, [ctypes.c_uint, ctypes.c_uint, ctypes.c_uint]),
     "impeller_ctx_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_void_p,
                                            ctypes.c_uint64, ctypes.c_int]),
+    "impeller_ctx_create_curve": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_void_p,
+                                                 ctypes.c_uint64, ctypes.c_int, ctypes.c_uint]),
     "impeller_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "impeller_ctx_points": (ctypes.c_void_p, [ctypes.c_void_p]),
     "impeller_ctx_len": (ctypes.c_uint64, [ctypes.c_void_p]),
@@ -66,10 +75,17 @@ SIGNATURES: dict[str, tuple] = {
                                             ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
     "impeller_gen_points": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                            ctypes.c_void_p]),
+    "impeller_gen_scalars_curve": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                                  ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                                  ctypes.c_void_p]),
+    "impeller_gen_points_curve": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                                 ctypes.c_uint64, ctypes.c_void_p]),
     "impeller_test_field_op": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
     "impeller_test_point_op": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_uint64, ctypes.c_void_p]),
+    "impeller_test_point_op_curve": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
     "impeller_ctx_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "impeller_ctx_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_uint32,
                                                  ctypes.POINTER(ctypes.c_uint32)]),

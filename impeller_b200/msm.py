@@ -30,6 +30,14 @@ from . import lib as _lib
 
 BN254_BITS = 254
 
+# Curves (include/impeller_msm.h IMPELLER_CURVE_*): the reference's MSM
+# library list covers bn254 (254-bit scalars) and bls12381 (255-bit scalars,
+# 381-bit base field), core/src/msm/xmake.lua and core/src/msm.rs:24-34.
+BN254, BLS12381 = 0, 1
+CURVE_NAMES = {BN254: "bn254", BLS12381: "bls12381"}
+SCALAR_BITS = {BN254: 254, BLS12381: 255}
+POINT_WORDS = {BN254: 16, BLS12381: 24}  # affine point, u32 words
+
 
 def _u32pp(arrays: Sequence[np.ndarray]):
     arr = (_lib.c_u32p * len(arrays))()
@@ -51,7 +59,14 @@ class MsmConfig:
     parts: int = 1
     stage_scalars: int = 1
     stage_points: int = 1
-    bits: int = BN254_BITS
+    bits: int | None = None  # scalar bits; None -> the curve's
+    curve: int = BN254
+
+    def __post_init__(self):
+        if self.curve not in CURVE_NAMES:
+            raise ValueError(f"unknown curve {self.curve}")
+        if self.bits is None:
+            self.bits = SCALAR_BITS[self.curve]
 
     def get_precompute(self) -> int:
         """common/src/msm_config.rs:17-25."""
@@ -62,7 +77,8 @@ class MsmConfig:
 
 def lib_name(config: MsmConfig) -> str:
     """core/src/msm.rs:101-112: msm_{curve}_{window}_{target}_{debug}."""
-    return f"msm_bn254_{config.window_size}_{config.target_window}_{'true' if config.debug else 'false'}"
+    return (f"msm_{CURVE_NAMES[config.curve]}_{config.window_size}_{config.target_window}_"
+            f"{'true' if config.debug else 'false'}")
 
 
 _shims: dict[str, ctypes.CDLL] = {}
@@ -79,7 +95,7 @@ def load_msm_library(config: MsmConfig) -> ctypes.CDLL:
         return _shims[name]
     core = _lib.load()  # the shim resolves impeller_msm_cfg from here
     from . import build as _build
-    path = _build.build_shim(config.window_size, config.target_window, config.debug)
+    path = _build.build_shim(config.window_size, config.target_window, config.debug, config.curve)
     L = ctypes.CDLL(path)
     for sym in ("msm", "msm_precompute"):
         fn = getattr(L, sym)
@@ -89,7 +105,8 @@ def load_msm_library(config: MsmConfig) -> ctypes.CDLL:
     return L
 
 
-def get_best_config(length: int, batches: int, mem_limit: int, cards: Sequence[int] = (0,)) -> MsmConfig:
+def get_best_config(length: int, batches: int, mem_limit: int, cards: Sequence[int] = (0,),
+                    curve: int = BN254) -> MsmConfig:
     """core/src/msm.rs:36-99: pick (window, target window, parts,
     batch_per_run) for `batches` MSMs of `length` points under `mem_limit`
     bytes of device memory.  The window comes from the autotune table; no
@@ -97,12 +114,13 @@ def get_best_config(length: int, batches: int, mem_limit: int, cards: Sequence[i
     batch_per_run and the fewest parts whose scratch fits."""
     L = _lib.load()
     c = int(L.impeller_default_window(max(1, length)))
-    W = -(-BN254_BITS // c)
+    W = window_count(c, curve)
     parts = 1
     while True:
         for bpr in range(min(batches, 8), 0, -1):
             cfg = MsmConfig(window_size=c, target_window=W, cards=list(cards), batch_per_run=bpr, parts=parts,
-                            stage_scalars=1 if parts == 1 else 2, stage_points=1 if parts == 1 else 2)
+                            stage_scalars=1 if parts == 1 else 2, stage_points=1 if parts == 1 else 2,
+                            curve=curve)
             if max(MSM(cfg).get_buffer_size(length)) <= mem_limit:
                 return cfg
         parts *= 2
@@ -116,7 +134,7 @@ def get_best_config(length: int, batches: int, mem_limit: int, cards: Sequence[i
 
 @dataclass
 class PointArray:
-    values: np.ndarray  # (len, 16) uint32
+    values: np.ndarray  # (len, POINT_WORDS[curve]) uint32
 
     @property
     def len(self) -> int:
@@ -141,7 +159,7 @@ class GpuBuffer:
 
 @dataclass
 class Point:
-    value: np.ndarray = field(default_factory=lambda: np.zeros(16, dtype=np.uint32))
+    value: np.ndarray = field(default_factory=lambda: np.zeros(16, dtype=np.uint32))  # resized to the curve's
 
 
 def alloc_gpu_buffer(size: int, device: int = 0):
@@ -158,7 +176,8 @@ class MSM:
         self.config = config
         if library is not None:
             self.lib = library
-        elif config.window_size == 16 and config.target_window == 16 and not config.debug:
+        elif (config.window_size == 16 and config.target_window == 16 and not config.debug
+              and config.curve == BN254):
             self.lib = _lib.load()  # the default symbols of the core library
         else:
             self.lib = load_msm_library(config)
@@ -193,7 +212,7 @@ class MSM:
                 h_scalars.append(np.ascontiguousarray(v.values, dtype=np.uint32))
             buffers, answers = mut_var[:len(cfg.cards)], mut_var[len(cfg.cards):]
             bufs = (ctypes.c_void_p * len(buffers))(*[b.ptr for b in buffers])
-            results = [np.zeros(16, dtype=np.uint32) for _ in answers]
+            results = [np.zeros(POINT_WORDS[cfg.curve], dtype=np.uint32) for _ in answers]
             cards = [gpu_mapping(c) for c in cfg.cards]
             rc = c_func(bufs, None, length, cfg.batch_per_run, cfg.parts, cfg.stage_scalars, cfg.stage_points,
                         len(cards), (ctypes.c_uint * len(cards))(*cards), _u32pp(h_points), batches,
@@ -220,7 +239,8 @@ class MSMPrecompute:
         self.config = config
         if library is not None:
             self.lib = library
-        elif config.window_size == 16 and config.target_window == 16 and not config.debug:
+        elif (config.window_size == 16 and config.target_window == 16 and not config.debug
+              and config.curve == BN254):
             self.lib = _lib.load()
         else:
             self.lib = load_msm_library(config)
@@ -261,20 +281,21 @@ def _stream_handle(stream) -> int | None:
     return getattr(stream, "cuda_stream", stream)
 
 
-def gen_points_device(n: int, seed: int = 0, start: int = 0, device: int = 0, stream=None):
+def gen_points_device(n: int, seed: int = 0, start: int = 0, device: int = 0, stream=None, curve: int = BN254):
     import torch
-    out = torch.empty((n, 16), dtype=torch.int32, device=f"cuda:{device}")
-    _lib.check(_lib.load().impeller_gen_points(out.data_ptr(), n, seed, start, _stream_handle(stream)),
+    out = torch.empty((n, POINT_WORDS[curve]), dtype=torch.int32, device=f"cuda:{device}")
+    _lib.check(_lib.load().impeller_gen_points_curve(curve, out.data_ptr(), n, seed, start, _stream_handle(stream)),
                "impeller_gen_points")
     return out
 
 
 def gen_scalars_device(n: int, seed: int = 0, stream_id: int = 1, dist: int = 0, start: int = 0, mont: bool = True,
-                       device: int = 0, stream=None):
+                       device: int = 0, stream=None, curve: int = BN254):
     import torch
     out = torch.empty((n, 8), dtype=torch.int32, device=f"cuda:{device}")
-    _lib.check(_lib.load().impeller_gen_scalars(out.data_ptr(), n, seed, stream_id, dist, start, 1 if mont else 0,
-                                                _stream_handle(stream)), "impeller_gen_scalars")
+    _lib.check(_lib.load().impeller_gen_scalars_curve(curve, out.data_ptr(), n, seed, stream_id, dist, start,
+                                                      1 if mont else 0, _stream_handle(stream)),
+               "impeller_gen_scalars")
     return out
 
 
@@ -310,18 +331,22 @@ def table_window(n: int) -> int:
 class MsmContext:
     """Points uploaded once and kept in HBM; MSMs over prefixes of them."""
 
-    def __init__(self, points, device: int = 0):
+    def __init__(self, points, device: int = 0, curve: int = BN254):
         L = _lib.load()
         self.device = device
+        self.curve = curve
+        self.pw = POINT_WORDS[curve]
         h = ctypes.c_void_p()
         if hasattr(points, "data_ptr"):
             self._points_ref = points  # borrowed device tensor, keep alive
-            n = points.shape[0]
-            _lib.check(L.impeller_ctx_create(ctypes.byref(h), device, points.data_ptr(), n, 1), "impeller_ctx_create")
+            n = points.numel() // self.pw
+            _lib.check(L.impeller_ctx_create_curve(ctypes.byref(h), device, points.data_ptr(), n, 1, curve),
+                       "impeller_ctx_create")
         else:
             pts = np.ascontiguousarray(points, dtype=np.uint32)
-            n = pts.shape[0]
-            _lib.check(L.impeller_ctx_create(ctypes.byref(h), device, pts.ctypes.data, n, 0), "impeller_ctx_create")
+            n = pts.size // self.pw
+            _lib.check(L.impeller_ctx_create_curve(ctypes.byref(h), device, pts.ctypes.data, n, 0, curve),
+                       "impeller_ctx_create")
         self.handle = h
         self.len = n
 
@@ -347,14 +372,14 @@ class MsmContext:
         import torch
         n = d_scalars.shape[0] if n is None else n
         if out is None:
-            out = torch.empty(16, dtype=torch.int32, device=f"cuda:{self.device}")
+            out = torch.empty(self.pw, dtype=torch.int32, device=f"cuda:{self.device}")
         _lib.check(_lib.load().impeller_msm_device(self.handle, d_scalars.data_ptr(), n, c, out.data_ptr(),
                                                    _stream_handle(stream)), "impeller_msm_device")
         return out
 
     def msm_host(self, h_scalars: np.ndarray, c: int = 0, stream=None) -> np.ndarray:
         sc = np.ascontiguousarray(h_scalars, dtype=np.uint32)
-        out = np.zeros(16, dtype=np.uint32)
+        out = np.zeros(self.pw, dtype=np.uint32)
         _lib.check(_lib.load().impeller_msm_host(self.handle, sc.ctypes.data, sc.shape[0], c, out.ctypes.data,
                                                  _stream_handle(stream)), "impeller_msm_host")
         return out
@@ -387,7 +412,7 @@ class MsmBatch:
         import torch
         cnt = len(self.sizes)
         if out is None:
-            out = torch.empty((cnt, 16), dtype=torch.int32, device=f"cuda:{self.ctx.device}")
+            out = torch.empty((cnt, self.ctx.pw), dtype=torch.int32, device=f"cuda:{self.ctx.device}")
         ptrs = (ctypes.c_void_p * cnt)(*[s.data_ptr() for s in d_scalars])
         _lib.check(_lib.load().impeller_batch_run(self.handle, ptrs, out.data_ptr(), _stream_handle(stream)),
                    "impeller_batch_run")
@@ -405,12 +430,13 @@ class MsmBatch:
             pass
 
 
-def n_precompute(window_size: int, target_window: int) -> int:
-    return int(_lib.load().impeller_msm_n_precompute(window_size, target_window))
+def n_precompute(window_size: int, target_window: int, curve: int = BN254) -> int:
+    return int(_lib.load().impeller_msm_n_precompute_curve(curve, window_size, target_window))
 
 
-def window_count(c: int) -> int:
-    return math.ceil(BN254_BITS / c)
+def window_count(c: int, curve: int = BN254) -> int:
+    """The reference's window count ceil(bits / c) (msm.cuh MsmConfig)."""
+    return math.ceil(SCALAR_BITS[curve] / c)
 
 
 # ------------------------------------------------------ continuous batching
@@ -428,7 +454,8 @@ class MsmServer:
 
     submit() queues a job and returns at once; jobs that arrive while others
     run are admitted as batch slots and HBM free up and run overlapped with
-    them; wait() returns the 16-word result and the job's latency."""
+    them; wait() returns the affine result (the context curve's point words)
+    and the job's latency."""
 
     def __init__(self, ctx: MsmContext, max_batch: int = 64, max_inflight: int = 3, hbm_budget: int = 0):
         L = _lib.load()
@@ -455,7 +482,7 @@ class MsmServer:
         return jid.value
 
     def wait(self, job: int):
-        out = np.zeros(16, dtype=np.uint32)
+        out = np.zeros(self.ctx.pw, dtype=np.uint32)
         lat = ctypes.c_double()
         rc = _lib.load().impeller_server_wait(self.handle, job, out.ctypes.data, ctypes.byref(lat))
         self._keep.pop(job, None)
@@ -463,7 +490,7 @@ class MsmServer:
         return out, lat.value
 
     def poll(self, job: int):
-        out = np.zeros(16, dtype=np.uint32)
+        out = np.zeros(self.ctx.pw, dtype=np.uint32)
         lat = ctypes.c_double()
         rc = _lib.load().impeller_server_poll(self.handle, job, out.ctypes.data, ctypes.byref(lat))
         if rc == 600:  # cudaErrorNotReady

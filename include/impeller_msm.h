@@ -66,6 +66,30 @@ cudaError_t impeller_msm_precompute_cfg(unsigned int window_size, unsigned int t
                                         unsigned long long len, unsigned int *const *h_points,
                                         unsigned int max_cards);
 
+/* Curves: the reference builds one MSM library per curve, MSM_CURVE = bn254
+ * or bls12381 (utils/expand_targets.py:40-41; Rust side core/src/msm.rs:24-34).
+ * BLS12-381 G1 points are 24 uint32 (x then y, 12 little-endian limbs each,
+ * Montgomery form), scalars 8 uint32 (Montgomery Fr), results 24 uint32. */
+#define IMPELLER_CURVE_BN254 0u
+#define IMPELLER_CURVE_BLS12381 1u
+
+/* msm() / msm_precompute() for a given curve (the per-curve libraries'
+ * symbols; the BLS12-381 shims libmsm_bls12381_{c}_{alpha}_{debug}.so forward
+ * here).  Configurations whose window count differs from the reference's
+ * table layout on that curve are refused (cudaErrorInvalidValue). */
+cudaError_t impeller_msm_cfg_curve(unsigned int curve, unsigned int window_size, unsigned int target_window,
+                                   int debug, void *const *buffers, unsigned long *buffer_sizes,
+                                   unsigned long long len, unsigned int batch_per_run, unsigned int parts,
+                                   unsigned int stage_scalers, unsigned int stage_points, unsigned int num_cards,
+                                   const unsigned int *cards, unsigned int const *const *h_points,
+                                   unsigned int batches, unsigned int const *const *h_scaler_batch,
+                                   unsigned int *const *h_result);
+cudaError_t impeller_msm_precompute_cfg_curve(unsigned int curve, unsigned int window_size,
+                                              unsigned int target_window, unsigned long long len,
+                                              unsigned int *const *h_points, unsigned int max_cards);
+unsigned int impeller_msm_n_precompute_curve(unsigned int curve, unsigned int window_size,
+                                             unsigned int target_window);
+
 /* Number of window tables the reference derives from (window_size,
  * target_window) for a 254-bit scalar (common/src/msm_config.rs:17-25). */
 unsigned int impeller_msm_n_precompute(unsigned int window_size, unsigned int target_window);
@@ -81,14 +105,19 @@ typedef struct impeller_ctx impeller_ctx;
  * borrows it and the caller keeps it alive. */
 cudaError_t impeller_ctx_create(impeller_ctx **out, int device, const uint32_t *points, uint64_t len,
                                 int points_on_device);
+/* The same on a given curve (IMPELLER_CURVE_*); every MSM, batch and server
+ * on the context then runs on that curve. */
+cudaError_t impeller_ctx_create_curve(impeller_ctx **out, int device, const uint32_t *points, uint64_t len,
+                                      int points_on_device, unsigned int curve);
 cudaError_t impeller_ctx_destroy(impeller_ctx *ctx);
-/* Device pointer of the resident points (len x 16 uint32). */
+/* Device pointer of the resident points (len x 16 uint32; len x 24 on
+ * BLS12-381). */
 const uint32_t *impeller_ctx_points(const impeller_ctx *ctx);
 uint64_t impeller_ctx_len(const impeller_ctx *ctx);
 
 /* Resident window tables for window size c (additive; the device-resident
- * counterpart of msm_precompute with one bucket set): W(c) = ceil(254/c)
- * tables of len points, table j = 2^(j*c) * P, kept in HBM next to the points.
+ * counterpart of msm_precompute with one bucket set): W(c) signed-digit
+ * windows (ceil(254/c) on BN254) tables of len points, table j = 2^(j*c) * P, kept in HBM next to the points.
  * MSMs on this context that use window c then accumulate every digit window
  * into one bucket set: no per-window reduction and no window doublings.
  * Replaces any previous tables.  Blocks until the tables are built. */
@@ -192,15 +221,25 @@ cudaError_t impeller_server_destroy(impeller_server *s);
 cudaError_t impeller_gen_scalars(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t stream, int dist,
                                  uint64_t start, int mont, cudaStream_t s);
 cudaError_t impeller_gen_points(uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t start, cudaStream_t s);
+/* The same streams on a given curve (IMPELLER_CURVE_*): scalars are 8 u32
+ * on both curves, points PW u32 (16 BN254, 24 BLS12-381), G the curve's
+ * generator. */
+cudaError_t impeller_gen_scalars_curve(int curve, uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t stream,
+                                       int dist, uint64_t start, int mont, cudaStream_t s);
+cudaError_t impeller_gen_points_curve(int curve, uint32_t *d_out, uint64_t n, uint64_t seed, uint64_t start,
+                                      cudaStream_t s);
 
 /* Element-wise field / point operations on the device, for parity tests.
- * field: 0 = Fq, 1 = Fr.  op: 0 add, 1 sub, 2 mul, 3 sqr, 4 neg, 5 to_mont,
+ * field: 0 = BN254 Fq, 1 = BN254 Fr, 2 = BLS12-381 Fq (12 u32 per element),
+ * 3 = BLS12-381 Fr.  op: 0 add, 1 sub, 2 mul, 3 sqr, 4 neg, 5 to_mont,
  * 6 from_mont, 7 inv (Fermat), 8 pow, 9 inv (binary extended Euclid).  Point ops (affine in/out): 0 add (madd path),
  * 1 dbl, 2 add via XYZZ+XYZZ, 3 k*P (k plain 256-bit). */
 cudaError_t impeller_test_field_op(int field, int op, const uint32_t *d_a, const uint32_t *d_b, uint32_t *d_out,
                                    uint64_t count, cudaStream_t s);
 cudaError_t impeller_test_point_op(int op, const uint32_t *d_p, const uint32_t *d_q, uint32_t *d_out,
                                    uint64_t count, cudaStream_t s);
+cudaError_t impeller_test_point_op_curve(int curve, int op, const uint32_t *d_p, const uint32_t *d_q, uint32_t *d_out,
+                                         uint64_t count, cudaStream_t s);
 
 /* Integer-multiply ceiling of `device`, measured: the throughput of
  * independent Fq Montgomery products (four chains per thread, full

@@ -32,7 +32,17 @@ P = 2188824287183927522224640574525727508869631115729782366268903789464522620858
 R_MOD = 21888242871839275222246405745257275088548364400416034343698204186575808495617
 MONT_R = 1 << 256
 
-FQ, FR = 0, 1
+# BLS12-381 (the reference's second curve): p (381 bits, 12 u32 limbs,
+# R = 2^384) and the group order r (255 bits, 8 limbs, R = 2^256).
+P_BLS = 0x1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f6241eabfffeb153ffffb9feffffffffaaab
+R_BLS = 0x73eda753299d7d483339d80809a1d80553bda402fffe5bfeffffffff00000001
+
+BN254, BLS12381 = 0, 1
+# per curve: symbol prefix, base modulus, scalar modulus, Fq words, Montgomery R of Fq
+CURVES = {BN254: ("orc_", P, R_MOD, 8, 1 << 256), BLS12381: ("orc_bls_", P_BLS, R_BLS, 12, 1 << 384)}
+
+# fields: BN254 Fq, Fr; BLS12-381 Fq, Fr
+FQ, FR, BLS_FQ, BLS_FR = 0, 1, 2, 3
 ADD, SUB, MUL, SQR, NEG, TO_MONT, FROM_MONT, INV, POW = range(9)
 PT_ADD, PT_DBL, PT_NEG, PT_SMUL, PT_ONCURVE = range(5)
 
@@ -55,14 +65,19 @@ def lib():
         if not os.path.exists(ORACLE_SO):
             subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
         L = ctypes.CDLL(ORACLE_SO)
-        L.orc_field_op.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_uint64]
-        L.orc_point_op.argtypes = [ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_uint64]
-        L.orc_gen_scalars.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64,
-                                      ctypes.c_uint64, ctypes.c_int, _u32p, ctypes.c_int]
-        L.orc_gen_points.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, _u32p, ctypes.c_int]
-        L.orc_msm_halo2.argtypes = [_u32p, _u32p, ctypes.c_uint64, _u32p, ctypes.c_int]
-        L.orc_msm_naive.argtypes = [_u32p, _u32p, ctypes.c_uint64, _u32p]
-        L.orc_precompute.argtypes = [_u32p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, _u32p]
+        for pre in ("orc_", "orc_bls_"):
+            getattr(L, pre + "field_op").argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p,
+                                                     ctypes.c_uint64]
+            getattr(L, pre + "point_op").argtypes = [ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_uint64]
+            getattr(L, pre + "gen_scalars").argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
+                                                        ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _u32p,
+                                                        ctypes.c_int]
+            getattr(L, pre + "gen_points").argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, _u32p,
+                                                       ctypes.c_int]
+            getattr(L, pre + "msm_halo2").argtypes = [_u32p, _u32p, ctypes.c_uint64, _u32p, ctypes.c_int]
+            getattr(L, pre + "msm_naive").argtypes = [_u32p, _u32p, ctypes.c_uint64, _u32p]
+            getattr(L, pre + "precompute").argtypes = [_u32p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                                       _u32p]
         _lib = L
     return _lib
 
@@ -80,6 +95,9 @@ def ref_lib():
         L.ref_point_add.argtypes = [_u32p, _u32p, _u32p, ctypes.c_uint64]
         L.ref_point_dbl.argtypes = [_u32p, _u32p, ctypes.c_uint64]
         L.ref_msm_naive.argtypes = [_u32p, _u32p, ctypes.c_uint64, _u32p]
+        L.ref_bls_point_add.argtypes = [_u32p, _u32p, _u32p, ctypes.c_uint64]
+        L.ref_bls_point_dbl.argtypes = [_u32p, _u32p, ctypes.c_uint64]
+        L.ref_bls_msm_naive.argtypes = [_u32p, _u32p, ctypes.c_uint64, _u32p]
         _ref = L
     return _ref
 
@@ -121,79 +139,118 @@ def from_mont(x: int, m: int) -> int:
 
 # ------------------------------------------------------------------- wrappers
 
+def _fn(curve: int, name: str):
+    return getattr(lib(), CURVES[curve][0] + name)
+
+
+def _pw(curve: int) -> int:
+    """u32 words per affine point."""
+    return 2 * CURVES[curve][3]
+
+
 def field_op(field: int, op: int, a: np.ndarray, b: np.ndarray | None = None, use_ref: bool = False) -> np.ndarray:
-    a = np.ascontiguousarray(a, dtype=np.uint32).reshape(-1, 8)
-    bb = None if b is None else np.ascontiguousarray(b, dtype=np.uint32).reshape(-1, 8)
+    """Element-wise field operation; field FQ / FR (BN254) or BLS_FQ / BLS_FR."""
+    words = 12 if field == BLS_FQ else 8
+    a = np.ascontiguousarray(a, dtype=np.uint32).reshape(-1, words)
+    bb = None if b is None else np.ascontiguousarray(b, dtype=np.uint32).reshape(-1, words)
     out = np.zeros_like(a)
-    L = ref_lib() if use_ref else lib()
-    fn = L.ref_field_op if use_ref else L.orc_field_op
-    rc = fn(field, op, _ptr(a), _ptr(bb), _ptr(out), a.shape[0])
+    if use_ref:
+        fn, f = ref_lib().ref_field_op, field
+    elif field in (BLS_FQ, BLS_FR):
+        fn, f = _fn(BLS12381, "field_op"), field - BLS_FQ
+    else:
+        fn, f = _fn(BN254, "field_op"), field
+    rc = fn(f, op, _ptr(a), _ptr(bb), _ptr(out), a.shape[0])
     if rc != 0:
         raise RuntimeError(f"field_op rc={rc}")
     return out
 
 
-def point_op(op: int, p: np.ndarray, q: np.ndarray | None = None) -> np.ndarray:
-    p = np.ascontiguousarray(p, dtype=np.uint32).reshape(-1, 16)
+def point_op(op: int, p: np.ndarray, q: np.ndarray | None = None, curve: int = BN254) -> np.ndarray:
+    pw = _pw(curve)
+    p = np.ascontiguousarray(p, dtype=np.uint32).reshape(-1, pw)
     qq = None
     if q is not None:
         qq = np.ascontiguousarray(q, dtype=np.uint32)
-        qq = qq.reshape(-1, 8) if op == PT_SMUL else qq.reshape(-1, 16)
+        qq = qq.reshape(-1, 8) if op == PT_SMUL else qq.reshape(-1, pw)
     out = np.zeros_like(p)
-    rc = lib().orc_point_op(op, _ptr(p), _ptr(qq), _ptr(out), p.shape[0])
+    rc = _fn(curve, "point_op")(op, _ptr(p), _ptr(qq), _ptr(out), p.shape[0])
     if rc != 0:
         raise RuntimeError(f"point_op rc={rc}")
     return out
 
 
 def gen_scalars(n: int, seed: int = 0, stream: int = 1, dist: int = DIST_UNIFORM, start: int = 0,
-                mont: bool = True, threads: int | None = None) -> np.ndarray:
+                mont: bool = True, threads: int | None = None, curve: int = BN254) -> np.ndarray:
     out = np.zeros((n, 8), dtype=np.uint32)
-    lib().orc_gen_scalars(seed, stream, dist, start, n, 1 if mont else 0, _ptr(out),
-                          threads or default_threads())
+    _fn(curve, "gen_scalars")(seed, stream, dist, start, n, 1 if mont else 0, _ptr(out), threads or default_threads())
     return out
 
 
-def gen_points(n: int, seed: int = 0, start: int = 0, threads: int | None = None) -> np.ndarray:
+def gen_points(n: int, seed: int = 0, start: int = 0, threads: int | None = None, curve: int = BN254) -> np.ndarray:
     """P_i = r_i * G, r_i the uniform Fr stream (seed, stream 0)."""
-    out = np.zeros((n, 16), dtype=np.uint32)
-    lib().orc_gen_points(seed, start, n, _ptr(out), threads or default_threads())
+    out = np.zeros((n, _pw(curve)), dtype=np.uint32)
+    _fn(curve, "gen_points")(seed, start, n, _ptr(out), threads or default_threads())
     return out
 
 
-def msm(points: np.ndarray, scalars: np.ndarray, threads: int | None = None) -> np.ndarray:
-    """halo2 best_multiexp restated; returns the canonical affine result (16 u32)."""
-    points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, 16)
+def msm(points: np.ndarray, scalars: np.ndarray, threads: int | None = None, curve: int = BN254) -> np.ndarray:
+    """halo2 best_multiexp restated; returns the canonical affine result."""
+    pw = _pw(curve)
+    points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, pw)
     scalars = np.ascontiguousarray(scalars, dtype=np.uint32).reshape(-1, 8)
     n = min(points.shape[0], scalars.shape[0])
     points, scalars = points[:n].copy(), scalars[:n].copy()
-    out = np.zeros(16, dtype=np.uint32)
-    lib().orc_msm_halo2(_ptr(points), _ptr(scalars), n, _ptr(out), threads or default_threads())
+    out = np.zeros(pw, dtype=np.uint32)
+    _fn(curve, "msm_halo2")(_ptr(points), _ptr(scalars), n, _ptr(out), threads or default_threads())
     return out
 
 
-def msm_naive(points: np.ndarray, scalars: np.ndarray) -> np.ndarray:
-    points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, 16)
+def msm_naive(points: np.ndarray, scalars: np.ndarray, curve: int = BN254) -> np.ndarray:
+    pw = _pw(curve)
+    points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, pw)
     scalars = np.ascontiguousarray(scalars, dtype=np.uint32).reshape(-1, 8)
-    out = np.zeros(16, dtype=np.uint32)
-    lib().orc_msm_naive(_ptr(points), _ptr(scalars), points.shape[0], _ptr(out))
+    out = np.zeros(pw, dtype=np.uint32)
+    _fn(curve, "msm_naive")(_ptr(points), _ptr(scalars), points.shape[0], _ptr(out))
     return out
 
 
-def ref_msm_naive(points: np.ndarray, scalars: np.ndarray) -> np.ndarray:
-    points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, 16)
+def ref_point_op(op: int, p: np.ndarray, q: np.ndarray | None = None, curve: int = BN254) -> np.ndarray:
+    """PT_ADD / PT_DBL on affine points through the reference's own
+    arithmetic (core/src/common/curve/src/curve_xyzz.cuh)."""
+    pw = _pw(curve)
+    p = np.ascontiguousarray(p, dtype=np.uint32).reshape(-1, pw)
+    out = np.zeros_like(p)
+    L = ref_lib()
+    add, dbl = (L.ref_point_add, L.ref_point_dbl) if curve == BN254 else (L.ref_bls_point_add, L.ref_bls_point_dbl)
+    if op == PT_ADD:
+        q = np.ascontiguousarray(q, dtype=np.uint32).reshape(-1, pw)
+        add(_ptr(p), _ptr(q), _ptr(out), p.shape[0])
+    elif op == PT_DBL:
+        dbl(_ptr(p), _ptr(out), p.shape[0])
+    else:
+        raise ValueError(op)
+    return out
+
+
+def ref_msm_naive(points: np.ndarray, scalars: np.ndarray, curve: int = BN254) -> np.ndarray:
+    """Double-and-add MSM through the reference's own host arithmetic."""
+    pw = _pw(curve)
+    points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, pw)
     scalars = np.ascontiguousarray(scalars, dtype=np.uint32).reshape(-1, 8)
-    out = np.zeros(16, dtype=np.uint32)
-    ref_lib().ref_msm_naive(_ptr(points), _ptr(scalars), points.shape[0], _ptr(out))
+    out = np.zeros(pw, dtype=np.uint32)
+    fn = ref_lib().ref_msm_naive if curve == BN254 else ref_lib().ref_bls_msm_naive
+    fn(_ptr(points), _ptr(scalars), points.shape[0], _ptr(out))
     return out
 
 
-def precompute(points: np.ndarray, shift: int, n_tables: int) -> np.ndarray:
+def precompute(points: np.ndarray, shift: int, n_tables: int, curve: int = BN254) -> np.ndarray:
     """Tables of core/src/msm/src/msm_impl.cuh:358-371: out[j] = 2^(j*shift) * P."""
-    points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, 16)
+    pw = _pw(curve)
+    points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, pw)
     n = points.shape[0]
-    out = np.zeros((n_tables, n, 16), dtype=np.uint32)
-    lib().orc_precompute(_ptr(points), n, shift, n_tables, _ptr(out))
+    out = np.zeros((n_tables, n, pw), dtype=np.uint32)
+    _fn(curve, "precompute")(_ptr(points), n, shift, n_tables, _ptr(out))
     return out
 
 
@@ -201,7 +258,7 @@ def precompute(points: np.ndarray, shift: int, n_tables: int) -> np.ndarray:
 # Small affine arithmetic over Python integers (canonical, non-Montgomery),
 # used to cross-check the C oracle on tiny inputs.
 
-def py_add(p1, p2):
+def py_add(p1, p2, p: int = P):
     if p1 is None:
         return p2
     if p2 is None:
@@ -209,42 +266,46 @@ def py_add(p1, p2):
     x1, y1 = p1
     x2, y2 = p2
     if x1 == x2:
-        if (y1 + y2) % P == 0:
+        if (y1 + y2) % p == 0:
             return None
-        lam = 3 * x1 * x1 * pow(2 * y1, -1, P) % P
+        lam = 3 * x1 * x1 * pow(2 * y1, -1, p) % p
     else:
-        lam = (y2 - y1) * pow(x2 - x1, -1, P) % P
-    x3 = (lam * lam - x1 - x2) % P
-    return x3, (lam * (x1 - x3) - y1) % P
+        lam = (y2 - y1) * pow(x2 - x1, -1, p) % p
+    x3 = (lam * lam - x1 - x2) % p
+    return x3, (lam * (x1 - x3) - y1) % p
 
 
-def py_mul(k: int, p):
+def py_mul(k: int, pt, p: int = P):
     acc = None
     while k:
         if k & 1:
-            acc = py_add(acc, p)
-        p = py_add(p, p)
+            acc = py_add(acc, pt, p)
+        pt = py_add(pt, pt, p)
         k >>= 1
     return acc
 
 
-def py_point_from_limbs(a) -> tuple | None:
-    a = np.asarray(a, dtype=np.uint32).reshape(16)
-    x, y = limbs_to_int(a[:8]), limbs_to_int(a[8:])
+def py_point_from_limbs(a, curve: int = BN254) -> tuple | None:
+    _, p, _, w, mr = CURVES[curve]
+    a = np.asarray(a, dtype=np.uint32).reshape(2 * w)
+    x, y = limbs_to_int(a[:w]), limbs_to_int(a[w:])
     if y == 0:
         return None
-    return from_mont(x, P), from_mont(y, P)
+    ri = pow(mr, -1, p)
+    return x * ri % p, y * ri % p
 
 
-def py_point_to_limbs(p) -> np.ndarray:
-    if p is None:
-        return np.zeros(16, dtype=np.uint32)
-    return np.concatenate([int_to_limbs(to_mont(p[0], P)), int_to_limbs(to_mont(p[1], P))])
+def py_point_to_limbs(pt, curve: int = BN254) -> np.ndarray:
+    _, p, _, w, mr = CURVES[curve]
+    if pt is None:
+        return np.zeros(2 * w, dtype=np.uint32)
+    return np.concatenate([int_to_limbs(pt[0] * mr % p, w), int_to_limbs(pt[1] * mr % p, w)])
 
 
-def py_msm(points: np.ndarray, scalars: np.ndarray) -> np.ndarray:
+def py_msm(points: np.ndarray, scalars: np.ndarray, curve: int = BN254) -> np.ndarray:
+    _, p, r, w, _ = CURVES[curve]
     acc = None
-    for pt, s in zip(np.asarray(points).reshape(-1, 16), np.asarray(scalars).reshape(-1, 8)):
-        k = from_mont(limbs_to_int(s), R_MOD)
-        acc = py_add(acc, py_mul(k, py_point_from_limbs(pt)))
-    return py_point_to_limbs(acc)
+    for pt, sc in zip(np.asarray(points).reshape(-1, 2 * w), np.asarray(scalars).reshape(-1, 8)):
+        k = from_mont(limbs_to_int(sc), r)
+        acc = py_add(acc, py_mul(k, py_point_from_limbs(pt, curve), p), p)
+    return py_point_to_limbs(acc, curve)

@@ -1,11 +1,11 @@
 """The reference's own GPU MSM, compiled for sm_100a (test and measurement
 infrastructure only).
 
-``_ref/libref_msm_bn254_<c>_<alpha>_false.so`` is the reference's
+``_ref/libref_msm_<curve>_<c>_<alpha>_false.so`` is the reference's
 ``core/src/msm/src/msm.cu`` built unmodified from its source tree by
-``oracle/Makefile`` (target ``ref_gpu``), one library per (window size,
-target window) exactly as the reference's ``Makefile.msm`` builds one per
-configuration.  This module drives it through its C ABI
+``oracle/Makefile`` (target ``ref_gpu``), one library per (curve, window
+size, target window) exactly as the reference's ``Makefile.msm`` builds one
+per configuration (curve ``bn254`` or ``bls12381``).  This module drives it through its C ABI
 (``core/src/msm/src/msm.h:4-11``) the way the reference's Rust operator does
 (``core/src/msm.rs:169-190, 282-366``; ``core/tests/msm.rs:150-240``):
 
@@ -14,7 +14,7 @@ configuration.  This module drives it through its C ABI
 * ``msm_precompute`` filling tables 1.. of pinned host point arrays from
   table 0, once;
 * blocking ``msm`` calls on pinned host points and scalars (Montgomery form),
-  16 u32 affine results.
+  affine results (16 u32 on BN254, 24 on BLS12-381).
 
 Only ``tests/`` (as a second parity pin, against the reference's real GPU
 output) and ``bench.py --impl reference`` (as the reference's B200 timing)
@@ -32,6 +32,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 LAMBDA = 254  # BN254 scalar bits (MSM_BITS)
+BN254, BLS12381 = 0, 1
+CURVE_NAMES = {BN254: "bn254", BLS12381: "bls12381"}
+CURVE_BITS = {BN254: 254, BLS12381: 255}  # MSM_BITS
+POINT_WORDS = {BN254: 16, BLS12381: 24}
 
 # (window size, target window): MsmConfig::default() and the reference cost
 # model's choice for n = 2^22 (core/src/msm/tuning/cost_model.py
@@ -41,17 +45,17 @@ TUNED_2E22_CONFIG = (17, 8)
 TUNED_2E22_PARTS = 16
 
 
-def lib_path(c: int, alpha: int) -> str:
-    return os.path.join(HERE, "_ref", f"libref_msm_bn254_{c}_{alpha}_false.so")
+def lib_path(c: int, alpha: int, curve: int = BN254) -> str:
+    return os.path.join(HERE, "_ref", f"libref_msm_{CURVE_NAMES[curve]}_{c}_{alpha}_false.so")
 
 
-def available(c: int = DEFAULT_CONFIG[0], alpha: int = DEFAULT_CONFIG[1]) -> bool:
-    return os.path.exists(lib_path(c, alpha))
+def available(c: int = DEFAULT_CONFIG[0], alpha: int = DEFAULT_CONFIG[1], curve: int = BN254) -> bool:
+    return os.path.exists(lib_path(c, alpha, curve))
 
 
-def n_precompute(c: int, alpha: int) -> int:
+def n_precompute(c: int, alpha: int, curve: int = BN254) -> int:
     """MsmConfig::get_precompute (common/src/msm_config.rs:17-25)."""
-    actual = -(-LAMBDA // c)
+    actual = -(-CURVE_BITS[curve] // c)
     n_windows = min(actual, alpha)
     return -(-actual // n_windows)
 
@@ -67,9 +71,10 @@ class RefGpuMsm:
     host memory (tables 1.. precomputed by the reference on the GPU)."""
 
     def __init__(self, points: np.ndarray, c: int = DEFAULT_CONFIG[0], alpha: int = DEFAULT_CONFIG[1],
-                 parts: int = 1, device: int = 0):
+                 parts: int = 1, device: int = 0, curve: int = BN254):
         import torch
-        path = lib_path(c, alpha)
+        path = lib_path(c, alpha, curve)
+        self.pw = pw = POINT_WORDS[curve]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} not built (make -C oracle ref_gpu needs the reference sources)")
         self.lib = ctypes.CDLL(path)
@@ -80,18 +85,18 @@ class RefGpuMsm:
                                  ctypes.c_uint, u32p, u32pp, ctypes.c_uint, u32pp, u32pp]
         self.lib.msm_precompute.restype = ctypes.c_int
         self.lib.msm_precompute.argtypes = [ctypes.c_ulonglong, u32pp, ctypes.c_uint]
-        points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, 16)
+        points = np.ascontiguousarray(points, dtype=np.uint32).reshape(-1, pw)
         self.n = points.shape[0]
         self.c, self.alpha, self.parts = c, alpha, parts
         # get_best_config: one scalar and one point stage for a single part, two otherwise
         self.stages = 1 if parts == 1 else 2
         self.device = device
         self.cards = (ctypes.c_uint32 * 1)(device)
-        self.k = n_precompute(c, alpha)
+        self.k = n_precompute(c, alpha, curve)
         self._tables = []
         ptrs = []
         for j in range(self.k):
-            t, a = _pinned_u32((self.n, 16))
+            t, a = _pinned_u32((self.n, pw))
             if j == 0:
                 a[:] = points
             self._tables.append((t, a))
@@ -110,10 +115,10 @@ class RefGpuMsm:
         self._buf = torch.empty(self.buffer_bytes, dtype=torch.uint8, device=f"cuda:{device}")
         self.buffers = (ctypes.c_void_p * 1)(self._buf.data_ptr())
         self._scal_t, self._scal = _pinned_u32((self.n, 8))
-        self._res_t, self._res = _pinned_u32((16,))
+        self._res_t, self._res = _pinned_u32((pw,))
 
     def tables(self) -> np.ndarray:
-        """The host point tables after the reference's precompute (k x n x 16)."""
+        """The host point tables after the reference's precompute (k x n x point words)."""
         return np.stack([a for _, a in self._tables])
 
     def load_scalars(self, scalars: np.ndarray) -> None:

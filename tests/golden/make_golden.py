@@ -21,6 +21,11 @@ the reference).
    the skewed witness-like mix).
 3. ``generators.json``: the first values of the seeded synthetic streams, so
    that any change to the input definitions is caught.
+4. ``msm_golden_bls12381.json`` / ``generators_bls12381.json``: the same for
+   the reference's second curve, BLS12-381 G1 (outputs from the reference's
+   host arithmetic, core/src/common/curve/src/bls12381.cuh over
+   core/src/common/mont/src/bls12381_fq.cuh / bls12381_fr.cuh).  The
+   reference ships no BLS12-381 known-answer vectors of its own.
 """
 from __future__ import annotations
 
@@ -131,6 +136,7 @@ def main(ref_root: str) -> None:
     with open(os.path.join(HERE, "msm_golden.json"), "w") as f:
         json.dump({"source": "outputs computed with oracle/_ref/libref_bn254.so (reference host arithmetic)",
                    "cases": cases}, f, indent=0)
+    bls_cases()
 
     gen = {
         "srs_points_seed0_first4": rows_hex(O.gen_points(4, seed=0)),
@@ -142,6 +148,51 @@ def main(ref_root: str) -> None:
     with open(os.path.join(HERE, "generators.json"), "w") as f:
         json.dump(gen, f, indent=1)
     print("wrote kat.json, msm_golden.json, generators.json")
+
+
+def bls_cases() -> None:
+    C = O.BLS12381
+    cases = []
+    r_minus_1 = O.int_to_limbs(O.to_mont(O.R_BLS - 1, O.R_BLS))
+    one_m = O.int_to_limbs(O.to_mont(1, O.R_BLS))
+
+    def add_case(name, pts, sc):
+        pts = np.ascontiguousarray(pts, dtype=np.uint32).reshape(-1, 24)
+        sc = np.ascontiguousarray(sc, dtype=np.uint32).reshape(-1, 8)
+        out = O.ref_msm_naive(pts, sc, curve=C)
+        cases.append({"name": name, "n": int(pts.shape[0]), "points": rows_hex(pts),
+                      "scalars": rows_hex(sc), "result": "".join(hexlimbs(out))})
+
+    pts = O.gen_points(128, seed=0, curve=C)
+    add_case("uniform_n1", pts[:1], O.gen_scalars(1, seed=0, stream=1, curve=C))
+    add_case("uniform_n9", pts[:9], O.gen_scalars(9, seed=0, stream=1, curve=C))
+    add_case("uniform_n128", pts, O.gen_scalars(128, seed=0, stream=1, curve=C))
+    add_case("skewed_n128", pts, O.gen_scalars(128, seed=0, stream=3, dist=O.DIST_SKEWED, curve=C))
+    add_case("zero_scalars_n8", pts[:8], np.zeros((8, 8), np.uint32))
+    neg = O.point_op(O.PT_NEG, pts[:1], curve=C)
+    add_case("p_and_minus_p", np.concatenate([pts[:1], neg]), np.stack([one_m, one_m]))
+    add_case("repeated_point_n17", np.repeat(pts[:1], 17, axis=0), O.gen_scalars(17, seed=0, stream=4, curve=C))
+    add_case("scalar_r_minus_1_n4", pts[:4], np.repeat(r_minus_1[None, :], 4, axis=0))
+    ident = pts[:24].copy()
+    ident[::5] = 0
+    add_case("identity_points_n24", ident, O.gen_scalars(24, seed=0, stream=5, curve=C))
+    mixed = O.gen_scalars(48, seed=0, stream=6, curve=C)
+    mixed[::3] = 0
+    mixed[1::7] = one_m
+    mixed[2::11] = r_minus_1
+    add_case("mixed_edges_n48", pts[:48], mixed)
+    with open(os.path.join(HERE, "msm_golden_bls12381.json"), "w") as f:
+        json.dump({"source": "outputs computed with oracle/_ref/libref_bn254.so ref_bls_msm_naive "
+                             "(reference host arithmetic, BLS12-381 G1)", "cases": cases}, f, indent=0)
+    gen = {
+        "srs_points_seed0_first4": rows_hex(O.gen_points(4, seed=0, curve=C)),
+        "srs_r_seed0_first4": rows_hex(O.gen_scalars(4, seed=0, stream=0, mont=False, curve=C)),
+        "uniform_seed0_stream1_first4_mont": rows_hex(O.gen_scalars(4, seed=0, stream=1, curve=C)),
+        "skewed_seed0_stream2_first32_canonical": rows_hex(
+            O.gen_scalars(32, seed=0, stream=2, dist=O.DIST_SKEWED, mont=False, curve=C)),
+    }
+    with open(os.path.join(HERE, "generators_bls12381.json"), "w") as f:
+        json.dump(gen, f, indent=1)
 
 
 if __name__ == "__main__":
