@@ -214,8 +214,79 @@ def run_reference(args, rank, world):
                          "sample": f"2^18-point prefix of the 2^{args.log2n} workload per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_gpu": gpu_leg,
+        "reference_gpu_ntt": reference_gpu_ntt(args),
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_ntt(args, log_n: int = 24) -> dict:
+    """The reference's own NTT kernels (core/src/ntt/src/ntt.cu built
+    unmodified for sm_100a, NTT_FIELD=bn254_fr) on 2^24 device-resident
+    BN254 Fr elements with the launch shape its operator uses ((8, 8),
+    core/src/ntt.rs:383-388), CUDA events.  Inputs and twiddles come from
+    the CPU oracle; nothing of this library runs here."""
+    try:
+        import ctypes as C
+        import torch
+        from oracle import oracle as O
+    except Exception as e:  # pragma: no cover
+        return {"unavailable": f"import failed: {e}"}
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_ntt_bn254_fr.so")
+    if not torch.cuda.is_available() or not os.path.exists(path):
+        return {"unavailable": "no CUDA device or reference NTT library not built"}
+
+    class PolyPtr(C.Structure):
+        _fields_ = [("ptr", C.c_void_p), ("len", C.c_size_t), ("rotate", C.c_size_t), ("offset", C.c_size_t),
+                    ("whole_len", C.c_size_t)]
+
+    ref = C.CDLL(path)
+    ref.ssip_ntt.restype = C.c_int
+    ref.ssip_ntt.argtypes = [PolyPtr, C.c_void_p, C.c_uint, C.c_void_p, C.c_uint, C.c_uint]
+    ref.recompute_ntt.restype = C.c_int
+    ref.recompute_ntt.argtypes = [PolyPtr, C.c_void_p, C.c_uint, C.c_void_p, C.c_uint, C.c_void_p, C.c_uint,
+                                  C.c_uint]
+    n = 1 << log_n
+    cores = os.cpu_count() or 1
+    x = torch.from_numpy(O.gen_scalars(n, seed=7, stream=11, threads=cores).view(np.int32)).cuda()
+    u = O.mont_limbs(O.root_of_unity(log_n))
+    tw = torch.from_numpy(O.ntt_roots(n // 2, u).view(np.int32)).cuda()
+    # pq_deg as the reference's GenPqOmegas::get_pq_len gives it for (8, 8) launch shapes
+    # (core/src/ntt.rs:340-355): max(deg_stage1, deg_stage2)
+    def get_deg(d, m):
+        r = 1
+        while True:
+            x = d if r == 1 else (d - 1) // r + 1
+            if x <= m:
+                return x
+            r += 1
+    deg = max(get_deg((log_n + 1) // 2, 9), get_deg(log_n // 2, 5))
+    pq, om = O.pq_omegas(deg, n, u)
+    d_pq = torch.from_numpy(pq.view(np.int32)).cuda()
+    d_om = torch.from_numpy(om.view(np.int32)).cuda()
+    stream = torch.cuda.current_stream()
+    p = PolyPtr(x.data_ptr(), n, 0, 0, n)
+
+    def timed(call):
+        for _ in range(max(3, args.warmup)):
+            if call() != 0:
+                raise RuntimeError("reference NTT call failed")
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    st = stream.cuda_stream
+    ms = timed(lambda: ref.ssip_ntt(p, tw.data_ptr(), log_n, st, 8, 8))
+    ms_re = timed(lambda: ref.recompute_ntt(p, d_pq.data_ptr(), deg, d_om.data_ptr(), log_n, st, 8, 8))
+    return {"workload": f"in-place forward NTT, BN254 Fr, n=2^{log_n}", "n": n, "unit": "elements/s",
+            "ssip_ntt": {"ms_per_step": ms, "value": n / (ms * 1e-3)},
+            "recompute_ntt": {"ms_per_step": ms_re, "value": n / (ms_re * 1e-3)},
+            "api": "reference ssip_ntt / recompute_ntt C ABI (core/src/ntt/src/ntt.h), CUDA events"}
 
 
 # ------------------------------------------------------------------ main
@@ -261,7 +332,7 @@ def main():
     ap.add_argument("--log2n", type=int, default=22)
     ap.add_argument("--no-extras", action="store_true", help="skip e2e / batched / CPU legs")
     ap.add_argument("--only", default="", help="comma list of extra legs to run (e2e, resident, batched, served, cpu, "
-                                               "bls12381); default all")
+                                               "bls12381, ntt); default all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -381,7 +452,8 @@ def main():
             "clocks": clocks,
         }
 
-    legs = set(args.only.split(",")) if args.only else {"e2e", "resident", "batched", "served", "cpu", "bls12381"}
+    legs = set(args.only.split(",")) if args.only else {"e2e", "resident", "batched", "served", "cpu", "bls12381",
+                                                         "ntt"}
     if not args.no_extras and rank == 0:
         if "e2e" in legs:
             line["e2e"] = e2e_reference_abi(M, pts[:n], scal[0], n, c, args)
@@ -401,6 +473,9 @@ def main():
         del pts
         torch.cuda.empty_cache()
         line["bls12381"] = bls12381_leg(M, dev, n, args)
+    if not args.no_extras and rank == 0 and "ntt" in legs:
+        torch.cuda.empty_cache()
+        line["ntt"] = ntt_leg(M, dev, args, peak.value)
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -434,6 +509,77 @@ def e2e_reference_abi(M, d_pts, d_scal, n, c, args) -> dict:
     del keep
     return {"value": n / dt, "unit": UNIT, "h2d_bytes_per_step": n * (64 + 32), "d2h_bytes_per_step": 64,
             "ms_per_step": dt * 1e3, "api": f"msm() C ABI ({M.lib_name(cfg)}), pinned host buffers, wall clock"}
+
+
+def ntt_leg(M, dev, args, imad_peak: float, log_n: int = 24) -> dict:
+    """The NTT operator (the reference's ssip_ntt / recompute_ntt, BN254 Fr):
+    one in-place forward transform of 2^24 device-resident elements per step,
+    CUDA events on the launching stream (512 MiB of data, > L2); the same
+    through host buffers (pinned polynomial uploaded and read back every
+    step); the recompute variant.  Roofline: Montgomery products per second
+    against the live integer-multiply ceiling, and HBM bytes moved."""
+    import torch
+    from impeller_b200 import ntt as NT
+    n = 1 << log_n
+    x = M.gen_scalars_device(n, seed=7, stream_id=11, device=dev)
+    w = NT.root_of_unity(log_n)
+    tw_h = np.zeros((n // 2, 8), np.uint32)
+    t0 = time.perf_counter()
+    NT.SsipPrecompute().get_fn()(tw_h, NT.to_mont_limbs(w))
+    precompute_s = time.perf_counter() - t0
+    tw = torch.from_numpy(tw_h.view(np.int32)).to(f"cuda:{dev}")
+    f = NT.SsipNtt().get_fn()
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms = timed(lambda: f(x, tw), args.steps)
+    g = NT.GenPqOmegas()
+    pq = np.zeros((g.get_pq_len(log_n), 8), np.uint32)
+    om = np.zeros((32, 8), np.uint32)
+    g.get_fn()(pq, om, n, NT.to_mont_limbs(w))
+    d_pq = torch.from_numpy(pq.view(np.int32)).to(f"cuda:{dev}")
+    d_om = torch.from_numpy(om.view(np.int32)).to(f"cuda:{dev}")
+    fr = NT.RecomputeNtt().get_fn()
+    ms_re = timed(lambda: fr(x, d_pq, d_om), args.steps)
+    # host buffers: upload, transform, read back
+    hx = torch.empty((n, 8), dtype=torch.int32, pin_memory=True)
+    hx.copy_(x.cpu())
+    ho = torch.empty_like(hx)
+
+    def e2e_step():
+        x.copy_(hx, non_blocking=True)
+        f(x, tw)
+        ho.copy_(x, non_blocking=True)
+
+    ms_e2e = timed(e2e_step, max(3, args.steps // 2))
+    prods = NT.butterfly_products(log_n) * PRODUCTS_PER_MUL
+    passes = NT.launches(log_n)
+    hbm_bytes = passes * 2 * 32 * n + 32 * n  # every pass reads and writes the data; twiddles about one more read
+    achieved = prods / (ms * 1e-3) / 1e9
+    return {"workload": f"in-place forward NTT, BN254 Fr, n=2^{log_n}, natural order", "n": n,
+            "value": n / (ms * 1e-3), "unit": "elements/s", "ms_per_step": ms,
+            "gpu_launches_per_step": passes, "twiddle_precompute_s": round(precompute_s, 3),
+            "recompute": {"ms_per_step": ms_re, "value": n / (ms_re * 1e-3)},
+            "e2e": {"value": n / (ms_e2e * 1e-3), "unit": "elements/s", "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": 32 * n,
+                    "api": "ssip_ntt C ABI between pinned-host copies, CUDA events"},
+            "roofline": {"bound": "imad", "kernel": "k_ntt_pass", "achieved": achieved, "peak": imad_peak,
+                         "unit": "G 32x32->64 products/s", "frac": achieved / imad_peak,
+                         "products_per_step": prods,
+                         "hbm_gbs_achieved": hbm_bytes / (ms * 1e-3) / 1e9,
+                         "peak_source": "impeller_imad_peak, measured live"}}
 
 
 def bls12381_leg(M, dev, n, args) -> dict:

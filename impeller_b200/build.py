@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-I" + os.path.join(ROOT, "include"),
            "-Wno-deprecated-gpu-targets"]
 
-SOURCES = ["engine.cu", "abi.cu", "aux_kernels.cu", "noalloc.cu", "serve.cu"]
+SOURCES = ["engine.cu", "abi.cu", "aux_kernels.cu", "noalloc.cu", "serve.cu", "ntt.cu"]
 
 
 def nvcc() -> str:
@@ -79,13 +79,17 @@ def build(verbose: bool = False, ptxas_v: bool = False, force: bool = False) -> 
             raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
         return obj, r.stdout + r.stderr
 
-    with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
-        results = list(ex.map(compile_one, SOURCES))
+    # an object is rebuilt when its source, a header or this script is newer
+    headers = [d for d in deps if not d.endswith(".cu")] + [os.path.abspath(__file__)]
+    todo = [src for src in SOURCES
+            if force or _stale(os.path.join(OBJ, src.replace(".cu", ".o")), [os.path.join(CSRC, src)] + headers)]
+    with cf.ThreadPoolExecutor(max_workers=max(1, len(todo))) as ex:
+        results = list(ex.map(compile_one, todo))
     if verbose or ptxas_v:
         for _, log in results:
             if log.strip():
                 print(log)
-    objs = [o for o, _ in results]
+    objs = [os.path.join(OBJ, src.replace(".cu", ".o")) for src in SOURCES]
     tmp = LIB + ".tmp"
     cmd = [cc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)

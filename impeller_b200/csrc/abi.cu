@@ -89,7 +89,13 @@ bool make_config(unsigned window_size, unsigned target_window, int debug, Config
     const u32 bits = curve == CURVE_BLS12381 ? 255u : 254u;
     const u32 ref_w = (bits + window_size - 1) / window_size;
     const u32 ref_nw = std::min(ref_w, target_window);
-    if ((ref_w + ref_nw - 1) / ref_nw != cfg.n_tables) {
+    const u32 ref_tables = (ref_w + ref_nw - 1) / ref_nw;
+    if (ref_tables == 1) {
+        // no window tables: every digit window gets its own bucket set
+        cfg.n_windows = cfg.W;
+        cfg.n_tables = 1;
+    }
+    if (ref_tables != cfg.n_tables) {
         set_error("window size " + std::to_string(window_size) + " with target window " +
                   std::to_string(target_window) +
                   " needs one more signed-digit window than the reference's table layout on this curve");

@@ -16,7 +16,22 @@ c_u32pp = ctypes.POINTER(c_u32p)
 c_void_pp = ctypes.POINTER(ctypes.c_void_p)
 c_ulong_p = ctypes.POINTER(ctypes.c_ulong)
 
-# Every symbol include/impeller_msm.h declares, with (restype, argtypes).
+
+class PolyPtr(ctypes.Structure):
+    """include/impeller_ntt.h PolyPtr (core/src/common/iter/src/iter.cuh:12-18)."""
+    _fields_ = [("ptr", ctypes.c_void_p), ("len", ctypes.c_size_t), ("rotate", ctypes.c_size_t),
+                ("offset", ctypes.c_size_t), ("whole_len", ctypes.c_size_t)]
+
+
+class PolySlice(ctypes.Structure):
+    """include/impeller_ntt.h PolySlice (core/src/common/slice/poly_slice.h:4-12)."""
+    _fields_ = [("begin", ctypes.c_ulonglong), ("slice_len", ctypes.c_ulonglong), ("len", ctypes.c_ulonglong)]
+
+
+_u32 = ctypes.c_uint
+_cptr = ctypes.c_void_p
+
+# Every symbol include/impeller_msm.h and include/impeller_ntt.h declare, with (restype, argtypes).
 SIGNATURES: dict[str, tuple] = {
     "msm": (ctypes.c_int, [c_void_pp, c_ulong_p, ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
                            ctypes.c_uint, ctypes.c_uint, c_u32p, c_u32pp, ctypes.c_uint, c_u32pp, c_u32pp]),
@@ -94,6 +109,18 @@ SIGNATURES: dict[str, tuple] = {
     "impeller_op_latency": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
     "impeller_msm_device_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                                    ctypes.c_void_p]),
+    "ssip_ntt": (ctypes.c_int, [PolyPtr, _cptr, _u32, _cptr, _u32, _u32]),
+    "ssip_precompute": (ctypes.c_int, [_cptr, _u32, _cptr]),
+    "recompute_ntt": (ctypes.c_int, [PolyPtr, _cptr, _u32, _cptr, _u32, _cptr, _u32, _u32]),
+    "gen_pq_omegas": (None, [_cptr, _cptr, _u32, _u32, _cptr]),
+    "distribute_powers": (ctypes.c_int, [PolyPtr, _cptr, ctypes.c_ulonglong, _cptr, ctypes.POINTER(PolySlice)]),
+    "impeller_ntt": (ctypes.c_int, [ctypes.c_int, PolyPtr, _cptr, _u32, _cptr]),
+    "impeller_ntt_precompute": (ctypes.c_int, [ctypes.c_int, _cptr, _u32, _cptr]),
+    "impeller_ntt_recompute": (ctypes.c_int, [ctypes.c_int, PolyPtr, _cptr, _u32, _cptr]),
+    "impeller_ntt_gen_pq_omegas": (ctypes.c_int, [ctypes.c_int, _cptr, _cptr, _u32, _u32, _cptr]),
+    "impeller_ntt_distribute_powers": (ctypes.c_int, [ctypes.c_int, PolyPtr, _cptr, ctypes.c_ulonglong, _cptr,
+                                                      ctypes.POINTER(PolySlice)]),
+    "impeller_ntt_launches": (_u32, [_u32]),
     "impeller_last_error": (ctypes.c_char_p, []),
     "impeller_version": (ctypes.c_char_p, []),
 }
@@ -130,17 +157,20 @@ def check(rc: int, what: str = "") -> None:
         raise ImpellerError(f"{what or 'impeller call'} failed with cudaError {rc}: {msg}")
 
 
+HEADERS = ("impeller_msm.h", "impeller_ntt.h")
+
+
 def declared_symbols(header: str | None = None) -> list[str]:
-    """Function names declared in include/impeller_msm.h."""
+    """Function names declared in include/impeller_msm.h and include/impeller_ntt.h
+    (or in one given header), in declaration order."""
     import re
-    header = header or os.path.join(os.path.dirname(HERE), "include", "impeller_msm.h")
-    text = open(header).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    names = re.findall(r"\b([A-Za-z_]\w*)\s*\(", text)
+    inc = os.path.join(os.path.dirname(HERE), "include")
     keep = []
-    for n in names:
-        if n in ("if", "sizeof", "defined") or n.isupper():
-            continue
-        if n not in keep:
+    for h in ([header] if header else [os.path.join(inc, name) for name in HEADERS]):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for n in re.findall(r"\b([A-Za-z_]\w*)\s*\(", text):
+            if n in ("if", "sizeof", "defined") or n.isupper() or n in keep:
+                continue
             keep.append(n)
-    return [n for n in keep if n.startswith(("msm", "impeller_"))]
+    return keep

@@ -66,6 +66,10 @@ def lib():
             subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
         L = ctypes.CDLL(ORACLE_SO)
         for pre in ("orc_", "orc_bls_"):
+            getattr(L, pre + "ntt").argtypes = [ctypes.c_int, _u32p, ctypes.c_uint32, _u32p]
+            getattr(L, pre + "ntt_roots").argtypes = [ctypes.c_int, _u32p, ctypes.c_uint64, _u32p]
+            getattr(L, pre + "pq_omegas").argtypes = [ctypes.c_int, _u32p, _u32p, ctypes.c_uint32, ctypes.c_uint64,
+                                                      _u32p]
             getattr(L, pre + "field_op").argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p,
                                                      ctypes.c_uint64]
             getattr(L, pre + "point_op").argtypes = [ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_uint64]
@@ -309,3 +313,78 @@ def py_msm(points: np.ndarray, scalars: np.ndarray, curve: int = BN254) -> np.nd
         k = from_mont(limbs_to_int(sc), r)
         acc = py_add(acc, py_mul(k, py_point_from_limbs(pt, curve), p), p)
     return py_point_to_limbs(acc, curve)
+
+
+# ------------------------------------------------------------------- NTT
+# The reference's NTT operator (core/src/ntt) over an 8-limb field:
+# BN254 Fr (its default NTT_FIELD), BN254 Fq or BLS12-381 Fr.
+
+NTT_FIELDS = {FR: (BN254, 1, R_MOD), FQ: (BN254, 0, P), BLS_FR: (BLS12381, 1, R_BLS)}
+
+
+def _ntt_fn(field: int, name: str):
+    curve, f, _ = NTT_FIELDS[field]
+    return _fn(curve, name), f
+
+
+def root_of_unity(log_n: int, field: int = FR) -> int:
+    """A primitive 2^log_n-th root of unity (canonical): g^((m-1)/2^log_n)
+    for the least quadratic non-residue g."""
+    m = NTT_FIELDS[field][2]
+    if (m - 1) % (1 << log_n):
+        raise ValueError("2^log_n does not divide m - 1")
+    g = 2
+    while pow(g, (m - 1) // 2, m) != m - 1:
+        g += 1
+    w = pow(g, (m - 1) >> log_n, m)
+    assert log_n == 0 or pow(w, 1 << (log_n - 1), m) == m - 1
+    return w
+
+
+def mont_limbs(v: int, field: int = FR) -> np.ndarray:
+    m = NTT_FIELDS[field][2]
+    return int_to_limbs(v * MONT_R % m)
+
+
+def ntt(x: np.ndarray, unit: np.ndarray, field: int = FR) -> np.ndarray:
+    """X[k] = sum_j x[j] unit^(j k), natural order (Montgomery in and out)."""
+    x = np.ascontiguousarray(x, dtype=np.uint32).reshape(-1, 8).copy()
+    n = x.shape[0]
+    log_n = n.bit_length() - 1
+    if n != 1 << log_n:
+        raise ValueError("length must be a power of two")
+    fn, f = _ntt_fn(field, "ntt")
+    u = np.ascontiguousarray(unit, dtype=np.uint32).reshape(8)
+    rc = fn(f, _ptr(x), log_n, _ptr(u))
+    if rc != 0:
+        raise RuntimeError(f"ntt rc={rc}")
+    return x
+
+
+def ntt_roots(length: int, unit: np.ndarray, field: int = FR) -> np.ndarray:
+    out = np.zeros((length, 8), dtype=np.uint32)
+    fn, f = _ntt_fn(field, "ntt_roots")
+    fn(f, _ptr(out), length, _ptr(np.ascontiguousarray(unit, dtype=np.uint32).reshape(8)))
+    return out
+
+
+def pq_omegas(pq_deg: int, length: int, unit: np.ndarray, field: int = FR):
+    pq = np.zeros(((1 << pq_deg) >> 1, 8), dtype=np.uint32)
+    om = np.zeros((32, 8), dtype=np.uint32)
+    fn, f = _ntt_fn(field, "pq_omegas")
+    rc = fn(f, _ptr(pq), _ptr(om), pq_deg, length, _ptr(np.ascontiguousarray(unit, dtype=np.uint32).reshape(8)))
+    if rc != 0:
+        raise RuntimeError(f"pq_omegas rc={rc}")
+    return pq, om
+
+
+def distribute_powers(x: np.ndarray, powers: np.ndarray, begin: int = 0, slice_len: int | None = None,
+                      poly_len: int | None = None, field: int = FR) -> np.ndarray:
+    """x[i] *= powers[((begin + i) % poly_len) % len(powers)]
+    (core/src/ntt/src/distribute_powers.cuh:5-11, PolySlice::to_origin)."""
+    x = np.ascontiguousarray(x, dtype=np.uint32).reshape(-1, 8)
+    powers = np.ascontiguousarray(powers, dtype=np.uint32).reshape(-1, 8)
+    n = x.shape[0]
+    poly_len = n if poly_len is None else poly_len
+    idx = ((begin + np.arange(n, dtype=np.uint64)) % np.uint64(poly_len)) % np.uint64(powers.shape[0])
+    return field_op(field, MUL, x, powers[idx.astype(np.int64)])
