@@ -128,6 +128,21 @@ def build_shim(window_size: int, target_window: int, debug: bool = False, curve:
     return out
 
 
+def ntt_library() -> str:
+    """lib/libntt.so, the name the reference's NTT operator loads
+    (core/src/ntt.rs:23, 98-106): a link to libimpeller_msm.so, which exports
+    ssip_ntt, ssip_precompute, recompute_ntt, gen_pq_omegas and
+    distribute_powers for BN254 Fr (the reference's default NTT_FIELD)."""
+    build()
+    os.makedirs(SHIM_DIR, exist_ok=True)
+    out = os.path.join(SHIM_DIR, "libntt.so")
+    if not os.path.islink(out):
+        if os.path.exists(out):
+            os.remove(out)
+        os.symlink(os.path.join("..", os.path.basename(LIB)), out)
+    return out
+
+
 if __name__ == "__main__":
     build(verbose="--verbose" in sys.argv, ptxas_v="--ptxas-v" in sys.argv, force="--force" in sys.argv)
     print(LIB)

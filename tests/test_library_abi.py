@@ -73,3 +73,25 @@ def test_window_table_roundtrip(L):
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(lib.ImpellerError):
         lib.load(str(tmp_path / "libimpeller_msm.so"))
+
+
+def test_ntt_library_name_and_symbols(L):
+    path = build.ntt_library()
+    assert os.path.basename(path) == "libntt.so"
+    S = ctypes.CDLL(path)
+    for sym in ("ssip_ntt", "ssip_precompute", "recompute_ntt", "gen_pq_omegas", "distribute_powers"):
+        assert getattr(S, sym)
+    assert L.impeller_ntt_launches(0) == 0
+    assert L.impeller_ntt_launches(11) == 1   # one tile, written out reversed
+    assert L.impeller_ntt_launches(20) == 3   # 9-bit pass, 11-bit pass, reorder
+    assert L.impeller_ntt_launches(24) == 4
+
+
+def test_bls_shim_name_and_config():
+    path = build.build_shim(16, 16, False, curve=M.BLS12381)
+    assert os.path.basename(path) == "libmsm_bls12381_16_16_false.so"
+    cfg = M.MsmConfig(curve=M.BLS12381)
+    assert cfg.bits == 255 and M.lib_name(cfg) == "msm_bls12381_16_16_false"
+    assert M.n_precompute(13, 4, curve=M.BLS12381) == 5
+    assert M.n_precompute(17, 5, curve=M.BLS12381) == 0  # needs a 16th window: refused
+    assert M.n_precompute(17, 15, curve=M.BLS12381) == 1
