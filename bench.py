@@ -556,7 +556,7 @@ def ntt_leg(M, dev, args, imad_peak: float, log_n: int = 24) -> dict:
     # host buffers: upload, transform, read back
     hx = torch.empty((n, 8), dtype=torch.int32, pin_memory=True)
     hx.copy_(x.cpu())
-    ho = torch.empty_like(hx)
+    ho = torch.empty((n, 8), dtype=torch.int32, pin_memory=True)
 
     def e2e_step():
         x.copy_(hx, non_blocking=True)

@@ -10,8 +10,9 @@
 //     bits: a CTA loads a tile of 2^(R + logC) elements (2^R points of the
 //     pass's digit times C = 2^logC consecutive low indices, so every global
 //     access is a run of C * 32 B) into shared memory, runs the R radix-2
-//     stages there with one Montgomery product per butterfly, and writes the
-//     tile back in place.  Tiles are disjoint, so passes are in place without
+//     stages there two at a time (a thread takes four elements through two
+//     stages between shared-memory round trips; one Montgomery product per
+//     butterfly), and writes the tile back in place.  Tiles are disjoint, so passes are in place without
 //     a scratch array.  The last pass takes the lowest 11 bits (a contiguous
 //     2048-element block);
 //   - one reordering pass (index bit reversal) with two 16 x 16 tiles per CTA
@@ -89,6 +90,8 @@ __device__ __forceinline__ Fe<F> twiddle(const u32 *tw, u32 e) {
 // global index (hi << (lo + R)) | (d << lo) | (low0 + c).  Stage s (global
 // bit, from lo + R - 1 down to lo) pairs d with d + 2^(s - lo):
 //   a' = a + b,  b' = (a - b) * w^((i mod 2^s) << (L - 1 - s)).
+// Stages go in pairs (s, s - 1); the two pairs of the lower stage share one
+// twiddle.  An odd last stage runs alone.
 // rev_out (only when the tile is the whole array): write element p to
 // position rev_L(p), canonical.
 template <class F, bool RECOMP>
@@ -112,18 +115,53 @@ k_ntt_pass(View v, const u32 *tw, u32 L, u32 lo, u32 R, u32 logC, int rev_out) {
     }
     __syncthreads();
 
-    for (int sl = (int)R - 1; sl >= 0; sl--) {
+    int sl = (int)R - 1;
+    while (sl >= 1) {
+        // two stages per round (index bits sl and sl - 1 of the digit): a
+        // thread loads four elements d0, d0 + h, d0 + 2h, d0 + 3h (h = 2^(sl-1))
         const u32 s = lo + (u32)sl;
-        const u32 lmask = (1u << sl) - 1;
+        const u32 h = 1u << (sl - 1);
+        const u32 hmask = h - 1;
+        for (u32 qd = threadIdx.x; qd < tsize / 4; qd += blockDim.x) {
+            const u32 c = qd & (C - 1);
+            const u32 q = qd >> logC;
+            const u32 d0 = ((q >> (sl - 1)) << (sl + 1)) | (q & hmask);
+            const u32 low = (u32)(low0 + c);
+            const u32 j0 = ((d0 & (2 * h - 1)) << lo) | low;  // i mod 2^s for d0 (bit sl-1 of d0 is 0)
+            const u32 ex0 = j0 << (L - 1 - s), ex1 = (j0 + (h << lo)) << (L - 1 - s);
+            const u32 ex2 = (((d0 & hmask) << lo) | low) << (L - s);
+            Fe<F> w0 = fe_one<F>(), w1 = fe_one<F>(), w2 = fe_one<F>();
+            if (ex0) w0 = twiddle<F, RECOMP>(tw, ex0);
+            w1 = twiddle<F, RECOMP>(tw, ex1);  // ex1 != 0: it has bit (lo + sl - 1) of j set
+            if (ex2) w2 = twiddle<F, RECOMP>(tw, ex2);
+            const u32 e0 = (d0 << logC) | c, eh = h << logC;
+            const Fe<F> x0 = smem_load<F>(ntt_smem, e0), x1 = smem_load<F>(ntt_smem, e0 + eh);
+            const Fe<F> x2 = smem_load<F>(ntt_smem, e0 + 2 * eh), x3 = smem_load<F>(ntt_smem, e0 + 3 * eh);
+            const Fe<F> a0 = fe_add<F>(x0, x2), a1 = fe_add<F>(x1, x3);
+            Fe<F> b0 = fe_sub<F>(x0, x2);
+            if (ex0) b0 = fe_mul<F>(b0, w0);
+            const Fe<F> b1 = fe_mul<F>(fe_sub<F>(x1, x3), w1);
+            Fe<F> y1 = fe_sub<F>(a0, a1), y3 = fe_sub<F>(b0, b1);
+            if (ex2) {
+                y1 = fe_mul<F>(y1, w2);
+                y3 = fe_mul<F>(y3, w2);
+            }
+            smem_store<F>(ntt_smem, e0, fe_add<F>(a0, a1));
+            smem_store<F>(ntt_smem, e0 + eh, y1);
+            smem_store<F>(ntt_smem, e0 + 2 * eh, fe_add<F>(b0, b1));
+            smem_store<F>(ntt_smem, e0 + 3 * eh, y3);
+        }
+        __syncthreads();
+        sl -= 2;
+    }
+    if (sl == 0) {
+        const u32 s = lo;
         for (u32 b = threadIdx.x; b < tsize / 2; b += blockDim.x) {
             const u32 c = b & (C - 1);
-            const u32 q = b >> logC;
-            const u32 d0 = ((q >> sl) << (sl + 1)) | (q & lmask);
-            const u32 e0 = (d0 << logC) | c, e1 = e0 + ((1u << sl) << logC);
+            const u32 e0 = ((b >> logC) << (logC + 1)) | c, e1 = e0 + C;
             const Fe<F> x = smem_load<F>(ntt_smem, e0), y = smem_load<F>(ntt_smem, e1);
             Fe<F> dif = fe_sub<F>(x, y);
-            const u32 j = ((d0 & lmask) << lo) | (u32)(low0 + c);  // i mod 2^s
-            const u32 ex = j << (L - 1 - s);
+            const u32 ex = ((u32)(low0 + c)) << (L - 1 - s);
             if (ex) dif = fe_mul<F>(dif, twiddle<F, RECOMP>(tw, ex));
             smem_store<F>(ntt_smem, e0, fe_add<F>(x, y));
             smem_store<F>(ntt_smem, e1, dif);

@@ -237,3 +237,37 @@ def butterfly_products(log_n: int) -> int:
     w^0 (n/2^(s+1) butterflies of stage s), i.e. n (log_n / 2 - 1) + 1."""
     n = 1 << log_n
     return sum(n // 2 - n // (2 << s) for s in range(log_n))
+
+
+if __name__ == "__main__":
+    # Profiling driver: python -m impeller_b200.ntt [log_n] [steps] [recompute]
+    # (one twiddle precompute, three warm-up transforms, then `steps` more).
+    import sys
+
+    import torch
+
+    from . import msm as _msm
+    log_n = int(sys.argv[1]) if len(sys.argv) > 1 else 24
+    steps = int(sys.argv[2]) if len(sys.argv) > 2 else 3
+    recompute = len(sys.argv) > 3 and sys.argv[3] == "recompute"
+    n = 1 << log_n
+    x = _msm.gen_scalars_device(n, seed=7, stream_id=11)
+    unit = to_mont_limbs(root_of_unity(log_n))
+    if recompute:
+        g = GenPqOmegas()
+        pq = np.zeros((g.get_pq_len(log_n), WORDS), np.uint32)
+        om = np.zeros((32, WORDS), np.uint32)
+        g.get_fn()(pq, om, n, unit)
+        d_pq, d_om = (torch.from_numpy(a.view(np.int32)).cuda() for a in (pq, om))
+        f = RecomputeNtt().get_fn()
+        run = lambda: f(x, d_pq, d_om)  # noqa: E731
+    else:
+        tw = np.zeros((n // 2, WORDS), np.uint32)
+        SsipPrecompute().get_fn()(tw, unit)
+        d_tw = torch.from_numpy(tw.view(np.int32)).cuda()
+        f = SsipNtt().get_fn()
+        run = lambda: f(x, d_tw)  # noqa: E731
+    for _ in range(3 + steps):
+        run()
+    torch.cuda.synchronize()
+    print(f"{3 + steps} transforms of 2^{log_n} done")

@@ -95,13 +95,13 @@ def test_rotated_and_sliced_views(N):
     x = rand_field(rng, n, O.R_MOD)
     tw = dev(twiddles(N, log_n))
     f = N.SsipNtt().get_fn()
-    # rotated by r: logical x'[i] = x[(n - r + i) mod n]
+    # rotated by r: logical element i is physical (n - r + i) mod n
     for r in (1, 5, n - 1):
         d = dev(x)
         f(d, tw, rotate=r)
         logical = np.roll(x, r, axis=0)
         want = O.ntt(logical, unit_for(log_n))
-        assert (np.roll(host(d), -r, axis=0) == want).all(), r
+        assert (np.roll(host(d), r, axis=0) == want).all(), r
     # a length-n slice of a longer array, wrapping around its end
     whole = n + 300
     big = rand_field(rng, whole, O.R_MOD)
