@@ -102,13 +102,15 @@ class ClockSampler:
 
 # ----------------------------------------------------------- algorithmics
 
-def signed_digit_stats(scalars_canonical: np.ndarray, c: int, shared: bool = False) -> tuple[int, int]:
+def signed_digit_stats(scalars_canonical: np.ndarray, c: int, shared: bool = False,
+                       windows: int | None = None) -> tuple[int, int]:
     """(nonzero signed digits, nonempty buckets) of the engine's recoding for
     canonical scalars (n x 8 u32): the entry count of the accumulate phase.
-    shared: every digit window uses one bucket set (resident window tables)."""
+    shared: every digit window uses one bucket set (resident window tables).
+    windows: digit windows (BN254 default ceil(254 / c))."""
     s = scalars_canonical.astype(np.uint64)
     words = [s[:, 2 * k] | (s[:, 2 * k + 1] << np.uint64(32)) for k in range(4)]
-    W = math.ceil(254 / c)
+    W = windows or math.ceil(254 / c)
     half = 1 << (c - 1)
     carry = np.zeros(s.shape[0], dtype=np.int64)
     nonzero, buckets = 0, 0
@@ -472,7 +474,7 @@ def main():
         ctx.close()
         del pts
         torch.cuda.empty_cache()
-        line["bls12381"] = bls12381_leg(M, dev, n, args)
+        line["bls12381"] = bls12381_leg(M, dev, n, args, peak.value)
     if not args.no_extras and rank == 0 and "ntt" in legs:
         torch.cuda.empty_cache()
         line["ntt"] = ntt_leg(M, dev, args, peak.value)
@@ -582,7 +584,7 @@ def ntt_leg(M, dev, args, imad_peak: float, log_n: int = 24) -> dict:
                          "peak_source": "impeller_imad_peak, measured live"}}
 
 
-def bls12381_leg(M, dev, n, args) -> dict:
+def bls12381_leg(M, dev, n, args, imad_peak: float) -> dict:
     """The same MSM on the reference's second curve, BLS12-381 G1 (381-bit
     base field in 12 limbs, 255-bit scalars): device-resident inputs timed
     with CUDA events (resident window tables where the autotune table puts
@@ -599,9 +601,12 @@ def bls12381_leg(M, dev, n, args) -> dict:
     c = ctx.window(n)
     outs = [torch.empty(24, dtype=torch.int32, device=f"cuda:{dev}") for _ in range(4)]
     stream = torch.cuda.current_stream()
+    from impeller_b200 import lib as L
+    lib = L.load()
     for w in range(args.warmup):
         ctx.msm_device(scal[w % 4], c=c, out=outs[w % 4])
     torch.cuda.synchronize()
+    lib.impeller_ctx_profile(ctx.handle, 1)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -610,7 +615,21 @@ def bls12381_leg(M, dev, n, args) -> dict:
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
+    phases = (ctypes.c_double * 8)()
+    runs = ctypes.c_uint32()
+    L.check(lib.impeller_ctx_profile_read(ctx.handle, phases, 8, ctypes.byref(runs)))
+    nr = max(1, runs.value)
+    phase_ms = {lib.impeller_phase_name(i).decode(): phases[i] / nr for i in range(8)}
     ctx.close()
+    # accumulate-phase roofline: 12-limb Montgomery products (12 rows of
+    # 12 + 1 + 12 partial products = 300) x 10 per mixed addition
+    W = math.ceil(255 / c) + (1 if c in (3, 5, 15, 17) else 0)
+    stats = [signed_digit_stats(M.to_host(M.gen_scalars_device(n, seed=0, stream_id=1 + v, mont=False, device=dev,
+                                                                curve=C)).reshape(n, 8), c, shared=bool(c_tab),
+                                windows=W) for v in range(4)]
+    madds = statistics.mean(nz - nb for nz, nb in stats)
+    acc_ms = phase_ms["accumulate"]
+    achieved = madds * MULS_PER_MADD * 300 / (acc_ms * 1e-3) / 1e9
     # drop-in ABI, host buffers
     cd = M.default_window(n)
     cfg = M.MsmConfig(window_size=cd, target_window=M.window_count(cd, C), curve=C)
@@ -632,6 +651,11 @@ def bls12381_leg(M, dev, n, args) -> dict:
     del keep
     return {"workload": f"single BLS12-381 G1 MSM, n=2^{int(math.log2(n))}, window c={c}",
             "window_tables": bool(c_tab), "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+            "roofline": {"bound": "imad", "kernel": "k_accumulate<Bls12381>", "achieved": achieved,
+                         "peak": imad_peak, "unit": "G 32x32->64 products/s", "frac": achieved / imad_peak,
+                         "per_launch": {"madds": madds, "products_per_madd": MULS_PER_MADD * 300, "ms": acc_ms},
+                         "peak_source": "impeller_imad_peak (8-limb Fq products), measured live"},
             "timing": "CUDA events, inputs resident, 4 rotating scalar vectors (> L2)",
             "e2e": {"value": n / dt, "unit": UNIT, "h2d_bytes_per_step": n * (96 + 32), "d2h_bytes_per_step": 96,
                     "ms_per_step": dt * 1e3, "api": f"msm() C ABI ({M.lib_name(cfg)}), pinned host buffers, "
