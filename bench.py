@@ -181,6 +181,16 @@ def reference_gpu(args, n: int, cores: int) -> dict:
         out[name] = {"window_size": c, "target_window": alpha, "parts": parts, "n_precompute": ref.k,
                      "ms_per_call": ms, "value": n / (ms / 1e3)}
         ref.close()
+    del pts, scal
+    if RG.available(16, 16, curve=RG.BLS12381):
+        # the same call on the reference's second curve (its msm.cu built for bls12381)
+        bp = O.gen_points(n, seed=0, threads=cores, curve=O.BLS12381)
+        bs = [O.gen_scalars(n, seed=0, stream=1 + v, threads=cores, curve=O.BLS12381) for v in range(2)]
+        ref = RG.RefGpuMsm(bp, 16, 16, curve=RG.BLS12381)
+        ms = ref.time_calls(bs, warmup=max(2, args.warmup), steps=args.steps)
+        out["bls12381_default"] = {"window_size": 16, "target_window": 16, "parts": 1, "ms_per_call": ms,
+                                   "value": n / (ms / 1e3)}
+        ref.close()
     return out
 
 
