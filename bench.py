@@ -641,7 +641,7 @@ def bls12381_leg(M, dev, n, args, imad_peak: float) -> dict:
     acc_ms = phase_ms["accumulate"]
     achieved = madds * MULS_PER_MADD * 300 / (acc_ms * 1e-3) / 1e9
     # drop-in ABI, host buffers
-    cd = M.default_window(n)
+    cd = M.default_window(n, C)
     cfg = M.MsmConfig(window_size=cd, target_window=M.window_count(cd, C), curve=C)
     op = M.MSM(cfg)
     buf, keep = M.alloc_gpu_buffer(op.get_buffer_size(n)[0], device=dev)

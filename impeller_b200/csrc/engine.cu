@@ -651,6 +651,17 @@ u32 default_window(u64 n) {
     return e ? e->c : model_window(n);
 }
 
+// The measured window table is BN254's.  On BLS12-381 (255-bit scalars) the
+// windows c = 3, 5, 15, 17 need one more signed-digit window whose digits
+// are only the carries out of the window below: every scalar lands in one
+// bucket of that window.  Move such a choice to the neighbouring window
+// without the extra one (16 for 15 and 17, which has no more windows).
+u32 curve_window(u32 c, u32 curve) {
+    if (curve != CURVE_BLS12381 || c < 3 || c > 31) return c;
+    if (digit_windows(c, curve) == (255u + c - 1u) / c) return c;
+    return c < 16 ? c + 1 : c - 1;
+}
+
 // Window of the resident tables the table recommends for MSMs of n points
 // (0: plain windows are faster at that size).
 u32 table_window(u64 n) {
@@ -678,7 +689,7 @@ u32 impeller::ctx_set_base(const impeller_ctx *ctx, u32 c) {
 u32 impeller::ctx_window(const impeller_ctx *ctx, u64 n) {
     const u32 ct = table_window(n);
     if (ct && ctx_set_base(ctx, ct) != NONE) return ct;
-    return default_window(n);
+    return curve_window(default_window(n), ctx->curve);
 }
 
 static cudaError_t ctx_reserve(impeller_ctx *ctx, size_t bytes, cudaStream_t st) {
@@ -722,6 +733,10 @@ const char *impeller_last_error(void) { return impeller::last_error(); }
 const char *impeller_version(void) { return "impeller-b200-msm 0.1 (sm_100a)"; }
 
 unsigned int impeller_default_window(uint64_t n) { return impeller::default_window(n); }
+
+unsigned int impeller_default_window_curve(uint64_t n, unsigned int curve) {
+    return impeller::curve_window(impeller::default_window(n), curve);
+}
 
 unsigned int impeller_table_window(uint64_t n) { return impeller::table_window(n); }
 

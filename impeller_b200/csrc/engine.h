@@ -44,6 +44,7 @@ struct MsmShape {
 u32 digit_windows(u32 c, u32 curve = CURVE_BN254);
 u32 default_window(u64 n);  // autotune table (or the cost model)
 u32 table_window(u64 n);    // tables window the autotune table recommends (0: none)
+u32 curve_window(u32 c, u32 curve);  // c moved off windows that need an extra digit window on the curve
 
 // Device property cache.
 int sm_count(int device);

@@ -60,6 +60,7 @@ SIGNATURES: dict[str, tuple] = {
     "impeller_ctx_precompute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint]),
     "impeller_ctx_window": (ctypes.c_uint, [ctypes.c_void_p, ctypes.c_uint64]),
     "impeller_default_window": (ctypes.c_uint, [ctypes.c_uint64]),
+    "impeller_default_window_curve": (ctypes.c_uint, [ctypes.c_uint64, ctypes.c_uint]),
     "impeller_table_window": (ctypes.c_uint, [ctypes.c_uint64]),
     "impeller_set_window_table": (ctypes.c_int, [c_u32p, c_u32p, c_u32p, ctypes.c_uint32]),
     "impeller_msm_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint,

@@ -113,7 +113,7 @@ def get_best_config(length: int, batches: int, mem_limit: int, cards: Sequence[i
     window tables (target_window = number of windows); the largest
     batch_per_run and the fewest parts whose scratch fits."""
     L = _lib.load()
-    c = int(L.impeller_default_window(max(1, length)))
+    c = int(L.impeller_default_window_curve(max(1, length), curve))
     W = window_count(c, curve)
     parts = 1
     while True:
@@ -318,8 +318,8 @@ def restore_default_window_table() -> None:
         set_window_table({})
 
 
-def default_window(n: int) -> int:
-    return int(_lib.load().impeller_default_window(n))
+def default_window(n: int, curve: int = BN254) -> int:
+    return int(_lib.load().impeller_default_window_curve(n, curve))
 
 
 def table_window(n: int) -> int:

@@ -127,6 +127,10 @@ unsigned int impeller_ctx_window(const impeller_ctx *ctx, uint64_t n);
 
 /* Window size the autotune table picks for a plain MSM of n points. */
 unsigned int impeller_default_window(uint64_t n);
+/* The same on a curve (IMPELLER_CURVE_*): on BLS12-381 a pick that would
+ * need an extra signed-digit window holding only carries (c = 3, 5, 15, 17)
+ * moves to its neighbour (4, 6, 16, 16). */
+unsigned int impeller_default_window_curve(uint64_t n, unsigned int curve);
 /* Window of resident tables the autotune table recommends for MSMs of n
  * points (0: the plain path is faster at that size). */
 unsigned int impeller_table_window(uint64_t n);

@@ -95,3 +95,11 @@ def test_bls_shim_name_and_config():
     assert M.n_precompute(13, 4, curve=M.BLS12381) == 5
     assert M.n_precompute(17, 5, curve=M.BLS12381) == 0  # needs a 16th window: refused
     assert M.n_precompute(17, 15, curve=M.BLS12381) == 1
+
+
+def test_bls_window_avoids_carry_only_windows(L):
+    for n in (1 << 10, 1 << 16, 1 << 18, 1 << 20, 1 << 22):
+        c = M.default_window(n)
+        cb = M.default_window(n, M.BLS12381)
+        assert cb not in (3, 5, 15, 17)
+        assert cb == c or (c, cb) in ((15, 16), (17, 16))
