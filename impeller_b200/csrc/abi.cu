@@ -23,7 +23,8 @@
 // accumulates all parts into one bucket set before reducing
 // (msm_impl.cuh:384-575).  With parts == 1 the whole card range stays
 // resident (later batch groups reuse the points) and is streamed in chunks
-// of about 2^20 points; with parts > 1 each part is a chunk, double-buffered
+// that start at 2^18 points and grow (stream_bounds); with parts > 1 each
+// part is a chunk, double-buffered
 // in two stages (the reference's stage_scalers / stage_points = 2 that
 // get_best_config pairs with parts > 1, core/src/msm.rs:89).
 #include <algorithm>
@@ -111,12 +112,30 @@ struct CardLayout {
     size_t o_images = 0, image_cap = 0, bytes = 0;  // streamed: one table image per chunk
 };
 
-// Chunks a resident (parts == 1) range of `len` points streams in: 1 (no
-// streaming) below 2^21 points, else about 2^20 points per chunk, at most 8.
-u32 stream_chunks(u64 len) {
-    const u64 k = len >> 20;
-    return k < 2 ? 1u : (u32)std::min<u64>(k, 8);
+// Chunk boundaries of a resident (parts == 1) range of `len` points that
+// streams in: one chunk (no streaming) below 2^21 points; else a first chunk
+// of 2^18 points, so that computing starts after a short upload, and chunks
+// growing by 7/4, about the ratio of a chunk's compute time to its upload
+// time, so that each chunk lands while the previous one is still being
+// computed.  A remainder under half the next size joins the last chunk.
+std::vector<u64> stream_bounds(u64 len) {
+    std::vector<u64> b{0};
+    if (len < (1ull << 21)) {
+        b.push_back(len);
+        return b;
+    }
+    u64 size = 1ull << 18, at = 0;
+    while (at < len) {
+        u64 take = std::min(size, len - at);
+        if (len - at - take < size / 2) take = len - at;
+        at += take;
+        b.push_back(at);
+        size = size * 7 / 4;
+    }
+    return b;
 }
+
+u32 stream_chunks(u64 len) { return (u32)stream_bounds(len).size() - 1; }
 
 // parts > 1: each part is a chunk, in one of two buffer stages.
 constexpr u32 PART_STAGES = 2;
@@ -274,9 +293,15 @@ cudaError_t run_card(CardJob &J) {
     const size_t point_stage = (size_t)cfg.n_tables * part_len * PW;  // u32 per stage
     EventPool events;
 
-    // chunk k covers points [k * chunk, ...) of the card range
-    const u64 chunk = staged ? part_len : (card_len + stream_chunks(card_len) - 1) / stream_chunks(card_len);
-    const u32 nchunks = card_len ? (u32)((card_len + chunk - 1) / chunk) : 0;
+    // chunk k covers points [bounds[k], bounds[k + 1]) of the card range
+    std::vector<u64> bounds;
+    if (staged) {
+        for (u64 at = 0; at < card_len; at += part_len) bounds.push_back(at);
+        bounds.push_back(card_len);
+    } else {
+        bounds = stream_bounds(card_len);
+    }
+    const u32 nchunks = card_len ? (u32)bounds.size() - 1 : 0;
 
     bool points_resident = false;
     for (u32 g = 0; g < J.batches; g += J.batch_per_run) {
@@ -284,7 +309,7 @@ cudaError_t run_card(CardJob &J) {
         if (card_len == 0) {
             // an empty range contributes the identity
             if (!multi)
-                for (u32 b = 0; b < M; b++) std::fill(J.h_result[g + b], J.h_result[g + b] + 16, 0u);
+                for (u32 b = 0; b < M; b++) std::fill(J.h_result[g + b], J.h_result[g + b] + cfg.PW, 0u);
             continue;
         }
         const int mode = multi ? 2 : 0;
@@ -332,8 +357,8 @@ cudaError_t run_card(CardJob &J) {
             }
             std::vector<Plan *> chunk_plan(nchunks, nullptr);
             for (u32 k = 0; k < nchunks; k++) {
-                const u64 s0 = (u64)k * chunk;
-                const u64 mk = std::min<u64>(chunk, card_len - s0);
+                const u64 s0 = bounds[k];
+                const u64 mk = bounds[k + 1] - s0;
                 const u32 slot = staged ? k % PART_STAGES : 0;
                 std::vector<const u32 *> sc(M);
                 for (u32 b = 0; b < M; b++)
@@ -355,8 +380,8 @@ cudaError_t run_card(CardJob &J) {
             for (auto &e : tl) cudaEventCreate(&e);
             Plan *plan = nullptr;
             for (u32 k = 0; k < nchunks; k++) {
-                const u64 s0 = (u64)k * chunk;
-                const u64 mk = std::min<u64>(chunk, card_len - s0);
+                const u64 s0 = bounds[k];
+                const u64 mk = bounds[k + 1] - s0;
                 const u32 slot = staged ? k % PART_STAGES : 0;
                 if (staged && k >= PART_STAGES) CK(cudaStreamWaitEvent(cs, computed[k - PART_STAGES], 0));
                 // points of this chunk: staged -> its stage buffer; resident -> in place
