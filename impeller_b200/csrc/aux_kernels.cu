@@ -166,30 +166,35 @@ __global__ void k_test_point(int op, const u32 *p, const u32 *q, u32 *out, u64 c
 }
 
 // Throughput ceiling of the Montgomery product itself: four independent
-// chains of Fq products per thread at full occupancy, nothing else in the
-// loop.  A product is 136 32x32 -> 64-bit partial products (64 for a*b, 64
-// for m*N, 8 reduction factors).
+// chains of base-field products per thread at full occupancy, nothing else
+// in the loop.  An N-limb product is 2 N^2 + N 32x32 -> 64-bit partial
+// products (N^2 for a*b, N^2 for m*p, N reduction factors): 136 for BN254's
+// 8 limbs, 300 for BLS12-381's 12.
+template <class F>
 __global__ void k_imad_peak(u32 *out, u32 iters, u32 seed) {
-    Fq acc[4], m;
+    constexpr int N = F::N;
+    constexpr Words<N> mod = words(F::M);
+    const u32 top = (1u << (31 - __clz(mod.v[N - 1]))) - 1u;  // keeps values below p
+    Fe<F> acc[4], m;
 #pragma unroll
-    for (int k = 0; k < 8; k++) m.l[k] = seed * (threadIdx.x + 5 * k + 1) + blockIdx.x;
-    m.l[7] &= 0x3fffffffu;  // below 2p
+    for (int k = 0; k < N; k++) m.l[k] = seed * (threadIdx.x + 5 * k + 1) + blockIdx.x;
+    m.l[N - 1] &= top;
 #pragma unroll
     for (int r = 0; r < 4; r++) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) acc[r].l[k] = m.l[(k + r) & 7] ^ (u32)r;
-        acc[r].l[7] &= 0x3fffffffu;
+        for (int k = 0; k < N; k++) acc[r].l[k] = m.l[(k + r) % N] ^ (u32)r;
+        acc[r].l[N - 1] &= top;
     }
 #pragma unroll 1
     for (u32 it = 0; it < iters; it++) {
 #pragma unroll
-        for (int r = 0; r < 4; r++) acc[r] = fe_mul<FqP>(acc[r], m);
+        for (int r = 0; r < 4; r++) acc[r] = fe_mul<F>(acc[r], m);
     }
     u32 v = 0;
 #pragma unroll
     for (int r = 0; r < 4; r++)
 #pragma unroll
-        for (int k = 0; k < 8; k++) v ^= acc[r].l[k];
+        for (int k = 0; k < N; k++) v ^= acc[r].l[k];
     if (v == 0x12345678u) out[blockIdx.x * blockDim.x + threadIdx.x] = v;
 }
 
@@ -221,6 +226,40 @@ cudaError_t launched(const char *what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) impeller::set_error(std::string("launch of ") + what + " failed: " + cudaGetErrorString(e));
     return e;
+}
+
+template <class F>
+cudaError_t imad_peak(int device, double *gops) {
+    if (!gops) return cudaErrorInvalidValue;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return e;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const u32 blocks = (u32)sms * 8, threads = 256, iters = F::N == 8 ? 1u << 11 : 1u << 10;
+    u32 *out = nullptr;
+    if ((e = cudaMalloc(&out, (size_t)blocks * threads * 4)) != cudaSuccess) return e;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    k_imad_peak<F><<<blocks, threads>>>(out, iters / 8, 7u);  // warm-up
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; rep++) {
+        cudaEventRecord(t0);
+        k_imad_peak<F><<<blocks, threads>>>(out, iters, 7u);
+        cudaEventRecord(t1);
+        cudaEventSynchronize(t1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t0, t1);
+        best = ms < best ? ms : best;
+    }
+    e = cudaGetLastError();
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaFree(out);
+    if (e != cudaSuccess) return e;
+    const double products = 2.0 * F::N * F::N + F::N;
+    *gops = (double)blocks * threads * iters * 4.0 * products / (best * 1e-3) / 1e9;
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -268,36 +307,13 @@ cudaError_t impeller_gen_points(uint32_t *d_out, uint64_t n, uint64_t seed, uint
     return impeller_gen_points_curve(IMPELLER_CURVE_BN254, d_out, n, seed, start, s);
 }
 
-cudaError_t impeller_imad_peak(int device, double *gops) {
-    if (!gops) return cudaErrorInvalidValue;
-    cudaError_t e = cudaSetDevice(device);
-    if (e != cudaSuccess) return e;
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const u32 blocks = (u32)sms * 8, threads = 256, iters = 1u << 11;
-    u32 *out = nullptr;
-    if ((e = cudaMalloc(&out, (size_t)blocks * threads * 4)) != cudaSuccess) return e;
-    cudaEvent_t t0, t1;
-    cudaEventCreate(&t0);
-    cudaEventCreate(&t1);
-    k_imad_peak<<<blocks, threads>>>(out, iters / 8, 7u);  // warm-up
-    float best = 1e30f;
-    for (int rep = 0; rep < 3; rep++) {
-        cudaEventRecord(t0);
-        k_imad_peak<<<blocks, threads>>>(out, iters, 7u);
-        cudaEventRecord(t1);
-        cudaEventSynchronize(t1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, t0, t1);
-        best = ms < best ? ms : best;
-    }
-    e = cudaGetLastError();
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
-    cudaFree(out);
-    if (e != cudaSuccess) return e;
-    *gops = (double)blocks * threads * iters * 4.0 * 136.0 / (best * 1e-3) / 1e9;
-    return cudaSuccess;
+cudaError_t impeller_imad_peak(int device, double *gops) { return imad_peak<FqP>(device, gops); }
+
+cudaError_t impeller_imad_peak_curve(int device, unsigned int curve, double *gops) {
+    if (curve == IMPELLER_CURVE_BLS12381) return imad_peak<BlsFqP>(device, gops);
+    if (curve == IMPELLER_CURVE_BN254) return imad_peak<FqP>(device, gops);
+    impeller::set_error("impeller_imad_peak_curve: unknown curve");
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t impeller_op_latency(int op, uint32_t iters, double *cycles_per_op) {

@@ -250,6 +250,9 @@ cudaError_t impeller_test_point_op_curve(int curve, int op, const uint32_t *d_p,
  * occupancy), in 10^9 32x32 -> 64-bit partial products per second (136 per
  * Montgomery product).  Blocks until done. */
 cudaError_t impeller_imad_peak(int device, double *gops);
+/* The same for a curve's base field (IMPELLER_CURVE_*): BLS12-381's 12-limb
+ * products count 300 partial products each. */
+cudaError_t impeller_imad_peak_curve(int device, unsigned int curve, double *gops);
 
 /* Single-thread latency, in SM clock cycles, of a dependent chain of one
  * operation: 0 Fq Montgomery product, 1 XYZZ addition (plus the doubling
