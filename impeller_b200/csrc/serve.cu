@@ -77,6 +77,7 @@ struct impeller_server {
     std::unordered_map<u64, Job> jobs;
     std::vector<std::unique_ptr<Batch>> inflight;
     std::vector<cudaStream_t> streams;
+    cudaMemPool_t pool = nullptr;  // batch scratch; keeps freed memory mapped for the next batch
     std::vector<u32 *> pinned;  // one result buffer per slot
     std::vector<void *> staging;  // one table-image buffer per slot
     size_t staging_cap = 0;
@@ -111,7 +112,7 @@ cudaError_t launch_batch(impeller_server *s, Batch &b, std::vector<Job *> &js, u
     b.bytes = o_plan + b.plan->scratch_bytes();
     b.stream = s->streams[slot];
     b.h_results = s->pinned[slot];
-    cudaError_t e = cudaMallocAsync(&b.mem, b.bytes, b.stream);
+    cudaError_t e = cudaMallocFromPoolAsync(&b.mem, b.bytes, s->pool, b.stream);
     if (e != cudaSuccess) return e;
     unsigned char *base = static_cast<unsigned char *>(b.mem);
     std::vector<const u32 *> sc(M);
@@ -249,6 +250,22 @@ cudaError_t impeller_server_create(impeller_server **out, impeller_ctx *ctx, uin
         hbm_budget = fr > reserve ? fr - reserve : fr / 2;
     }
     s->budget = hbm_budget;
+    {
+        // a pool of its own that returns nothing to the driver between batches
+        // (the default pool unmaps freed memory at every synchronisation,
+        // and mapping it again costs each batch time on the host)
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ctx->device;
+        if ((e = cudaMemPoolCreate(&s->pool, &props)) != cudaSuccess) return e;
+        uint64_t keep = hbm_budget;
+        if ((e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+            cudaMemPoolDestroy(s->pool);
+            s->pool = nullptr;
+            return e;
+        }
+    }
     for (u32 i = 0; i < max_inflight; i++) {
         cudaStream_t st;
         if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return e;
@@ -388,6 +405,7 @@ cudaError_t impeller_server_destroy(impeller_server *s) {
     }
     for (auto p : s->pinned) cudaFreeHost(p);
     for (auto p : s->staging) cudaFreeHost(p);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return cudaSuccess;
 }
