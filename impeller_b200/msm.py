@@ -517,3 +517,26 @@ class MsmServer:
             self.close()
         except Exception:
             pass
+
+
+if __name__ == "__main__":
+    # Profiling driver: python -m impeller_b200.msm [bn254|bls12381] [log_n] [table_c] [steps]
+    # (device-generated points and scalars, one resident table set for window
+    # table_c (0: plain windows), three warm-up MSMs, then `steps` more).
+    import sys
+
+    import torch
+    curve = {"bn254": BN254, "bls12381": BLS12381}[sys.argv[1] if len(sys.argv) > 1 else "bn254"]
+    log_n = int(sys.argv[2]) if len(sys.argv) > 2 else 20
+    table_c = int(sys.argv[3]) if len(sys.argv) > 3 else 20
+    steps = int(sys.argv[4]) if len(sys.argv) > 4 else 2
+    n = 1 << log_n
+    ctx = MsmContext(gen_points_device(n, seed=0, curve=curve), curve=curve)
+    if table_c:
+        ctx.precompute(table_c)
+    sc = gen_scalars_device(n, seed=0, stream_id=1, curve=curve)
+    for _ in range(3 + steps):
+        ctx.msm_device(sc, c=table_c)
+    torch.cuda.synchronize()
+    ctx.close()
+    print(f"{3 + steps} MSMs of 2^{log_n} on {CURVE_NAMES[curve]} done")
