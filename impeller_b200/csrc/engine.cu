@@ -73,6 +73,26 @@ int sm_count(int device) {
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// The sort-path rule of Plan::build, from the shapes alone: bins of FINE
+// buckets (at most SORT_MAX_BINS) times tiles of scalars (sized by the most
+// digit windows of any MSM) at most SORT_MAX_CELLS count cells.
+bool Plan::two_level_sort(const std::vector<MsmShape> &shapes) {
+    u64 nb = 0;
+    u32 wmax = 1;
+    for (const MsmShape &s : shapes) {
+        if (s.c < 3 || s.c > 31) return false;
+        const u32 W = digit_windows(s.c, s.curve);
+        const u32 nw = (s.n_windows == 0 || s.n_windows > W) ? W : s.n_windows;
+        nb += (u64)nw << (s.c - 1);
+        wmax = std::max(wmax, W);
+    }
+    const u32 tile = std::max(32u, std::min(1024u, (STAGE_ENTRIES / wmax) & ~31u));
+    u64 stiles = 0;
+    for (const MsmShape &s : shapes) stiles += (s.n + tile - 1) / tile;
+    const u64 nbins = (nb + FINE - 1) / FINE;
+    return stiles > 0 && nbins <= SORT_MAX_BINS && nbins * stiles <= SORT_MAX_CELLS;
+}
+
 bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     p.device = device;
     p.shapes = shapes;
@@ -211,7 +231,7 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     }
     tile_first[p.M] = (u32)stiles;
     const u64 nbins = (nb + FINE - 1) / FINE;
-    p.msd = stiles > 0 && nbins <= SORT_MAX_BINS && nbins * stiles <= (1ull << 26);
+    p.msd = stiles > 0 && nbins <= SORT_MAX_BINS && nbins * stiles <= SORT_MAX_CELLS;
     if (p.msd) {
         p.nbins = (u32)nbins;
         p.sort_tiles = (u32)stiles;

@@ -62,6 +62,10 @@ class Plan {
   public:
     // Every MSM reads points[table_base + (w / n_windows) * table_stride + i].
     static bool build(Plan &p, int device, const std::vector<MsmShape> &shapes);
+    // Whether a plan of these shapes would sort its entries with the
+    // two-level counting sort (fast) rather than the per-entry atomic sort
+    // that build() falls back to for very large batches.
+    static bool two_level_sort(const std::vector<MsmShape> &shapes);
     ~Plan();
 
     // Enqueue one run.  scalars[m] are device pointers.  carry_mode:

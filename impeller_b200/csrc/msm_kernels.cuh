@@ -184,6 +184,7 @@ __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ c
 static constexpr u32 FINE_BITS = 10;
 static constexpr u32 FINE = 1u << FINE_BITS;     // buckets per coarse bin
 static constexpr u32 SORT_MAX_BINS = 8192;       // nb <= 2^23
+static constexpr u64 SORT_MAX_CELLS = 1ull << 26;  // bins x scalar tiles (count matrix entries)
 static constexpr u32 STAGE_ENTRIES = 16384;      // staged entries per tile
 static constexpr u32 SEG_ENTRIES = 32768;        // entries per fine segment (staged whole)
 static constexpr u32 SORT_BLOCK = 512;

@@ -179,10 +179,18 @@ void dispatcher(impeller_server *s) {
         while (s->inflight.size() < s->max_inflight && !s->pending.empty()) {
             std::vector<Job *> js;
             std::vector<u64> ids;
+            std::vector<MsmShape> shapes;
             u64 bytes = 0;
             while (!s->pending.empty() && js.size() < s->max_batch) {
                 Job &j = s->jobs[s->pending.front()];
                 if (s->used + bytes + j.bytes > s->budget) break;
+                // keep the batch on the two-level sort: a batch past its
+                // limits sorts entry by entry, slower than its jobs alone
+                shapes.push_back(j.shape);
+                if (!js.empty() && !Plan::two_level_sort(shapes)) {
+                    shapes.pop_back();
+                    break;
+                }
                 bytes += j.bytes;
                 js.push_back(&j);
                 ids.push_back(s->pending.front());
