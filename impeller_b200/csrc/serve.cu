@@ -42,6 +42,10 @@ double now_s() {
 
 size_t up256(size_t x) { return (x + 255) / 256 * 256; }
 
+// Device memory a server maps for batch scratch when it starts (at most its
+// HBM budget).
+constexpr u64 POOL_RESERVE = 16ull << 30;
+
 struct Job {
     const u32 *h_scalars = nullptr;
     u64 n = 0;
@@ -287,6 +291,17 @@ cudaError_t impeller_server_create(impeller_server **out, impeller_ctx *ctx, uin
         s->staging_cap = (size_t)max_batch * 4096 + (1u << 20);  // descriptors, windows, reduce blocks
         if ((e = cudaHostAlloc(&t, s->staging_cap, cudaHostAllocPortable)) != cudaSuccess) return e;
         s->staging.push_back(t);
+    }
+    {
+        // Map the pool's memory now: growing it on demand under load took
+        // single batch launches 1-2 s (the host blocks while new memory is
+        // mapped), which turned bursts into backlogs.  The pool keeps what
+        // is freed (release threshold = budget), so this stays mapped.
+        void *warm = nullptr;
+        const size_t reserve = (size_t)std::min<u64>(s->budget, POOL_RESERVE);
+        if ((e = cudaMallocFromPoolAsync(&warm, reserve, s->pool, s->streams[0])) != cudaSuccess) return e;
+        if ((e = cudaFreeAsync(warm, s->streams[0])) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(s->streams[0])) != cudaSuccess) return e;
     }
     impeller_server *raw = s.release();
     raw->worker = std::thread(dispatcher, raw);

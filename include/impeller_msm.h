@@ -189,8 +189,10 @@ cudaError_t impeller_batch_profile_read(impeller_batch *b, double *ms_per_phase,
  * (at most max_batch jobs) runs as one batch on its own stream, so batches on
  * the GPU at the same time overlap.  Each job uses the window (and resident
  * table set) the context would use alone, so its result is the same alone and
- * in any mix.  The caller keeps h_scalars alive and unchanged until the job's
- * result has been taken.
+ * in any mix.  Batch scratch comes from a memory pool of the server's own,
+ * mapped at creation (16 GiB, or the budget if smaller) and kept mapped.  The
+ * caller keeps h_scalars alive and unchanged until the job's result has been
+ * taken.
  */
 typedef struct impeller_server impeller_server;
 typedef struct impeller_server_stats {
