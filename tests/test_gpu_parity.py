@@ -372,3 +372,23 @@ def test_resident_window_tables(M):
         assert (out[i] == O.msm(pts[:s], scal[i])).all(), s
     b.close()
     ctx.close()
+
+
+def test_resident_host_scalars_large(M):
+    # impeller_msm_host above 2^21 points: the result equals the
+    # device-scalar path's, plain and with a resident table set, and the
+    # oracle's
+    n = (1 << 21) + 12345
+    d = M.gen_points_device(n, seed=16)
+    ctx = M.MsmContext(d)
+    dsc = M.gen_scalars_device(n, seed=16, stream_id=1)
+    sc = M.to_host(dsc).reshape(n, 8)
+    got = ctx.msm_host(sc)
+    assert (got == host(ctx.msm_device(dsc))).all()
+    assert (got == O.msm(M.to_host(d).reshape(n, 16), sc)).all()
+    ctx.precompute(20)
+    for s, dist in ((2, O.DIST_UNIFORM), (3, O.DIST_SKEWED)):
+        dsc = M.gen_scalars_device(n, seed=16, stream_id=s, dist=dist)
+        for c in (0, 20, 16):
+            assert (ctx.msm_host(M.to_host(dsc).reshape(n, 8), c=c) == host(ctx.msm_device(dsc, c=c))).all(), (s, c)
+    ctx.close()
