@@ -179,11 +179,16 @@ def test_full_size_2e24_roundtrip(N):
     assert torch.equal(x, x0)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_NTT), reason="reference NTT library not built")
-@pytest.mark.parametrize("log_n", [10, 16, 20, 24])
-def test_matches_reference_gpu_kernels(N, log_n):
+REF_NTT_LIBS = {O.FR: REF_NTT, O.BLS_FR: os.path.join(os.path.dirname(O.__file__), "_ref", "libref_ntt_bls12381_fr.so")}
+
+
+@pytest.mark.parametrize("field,log_n", [(O.FR, 10), (O.FR, 16), (O.FR, 20), (O.FR, 24),
+                                         (O.BLS_FR, 12), (O.BLS_FR, 18), (O.BLS_FR, 22)])
+def test_matches_reference_gpu_kernels(N, field, log_n):
+    if not os.path.exists(REF_NTT_LIBS[field]):
+        pytest.skip("reference NTT library for this field not built")
     from impeller_b200 import lib
-    ref = ctypes.CDLL(REF_NTT)
+    ref = ctypes.CDLL(REF_NTT_LIBS[field])
     ref.ssip_ntt.restype = ctypes.c_int
     ref.ssip_ntt.argtypes = [lib.PolyPtr, ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p, ctypes.c_uint,
                              ctypes.c_uint]
@@ -193,22 +198,23 @@ def test_matches_reference_gpu_kernels(N, log_n):
     ref.ssip_precompute.restype = ctypes.c_int
     ref.ssip_precompute.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]
     n = 1 << log_n
+    nf = _nf(N, field)
     from impeller_b200 import msm as M
-    x = M.gen_scalars_device(n, seed=6, stream_id=log_n)
-    u = np.ascontiguousarray(unit_for(log_n))
+    x = M.gen_scalars_device(n, seed=6, stream_id=log_n, curve=M.BLS12381 if field == O.BLS_FR else M.BN254)
+    u = np.ascontiguousarray(unit_for(log_n, field))
     tw_ref = np.zeros((n // 2, 8), np.uint32)
     assert ref.ssip_precompute(tw_ref.ctypes.data, n // 2, u.ctypes.data) == 0
-    tw = twiddles(N, log_n)
+    tw = twiddles(N, log_n, field)
     assert (tw == tw_ref).all()
     d_tw = dev(tw)
     ours, theirs = x.clone(), x.clone()
-    N.SsipNtt().get_fn()(ours, d_tw)
+    N.SsipNtt(field=nf).get_fn()(ours, d_tw)
     torch.cuda.synchronize()
     assert ref.ssip_ntt(lib.PolyPtr(theirs.data_ptr(), n, 0, 0, n), d_tw.data_ptr(), log_n, None, 8, 8) == 0
     torch.cuda.synchronize()
     assert torch.equal(ours, theirs)
     # recompute variant, both libraries
-    g = N.GenPqOmegas()
+    g = N.GenPqOmegas(field=nf)
     pq = np.zeros((g.get_pq_len(log_n), 8), np.uint32)
     om = np.zeros((32, 8), np.uint32)
     g.get_fn()(pq, om, n, u)
@@ -219,8 +225,8 @@ def test_matches_reference_gpu_kernels(N, log_n):
                              log_n, None, 8, 8) == 0
     torch.cuda.synchronize()
     ours2 = x.clone()
-    N.RecomputeNtt().get_fn()(ours2, d_pq, d_om)
+    N.RecomputeNtt(field=nf).get_fn()(ours2, d_pq, d_om)
     torch.cuda.synchronize()
     assert torch.equal(theirs, ours) and torch.equal(ours2, ours)
     if log_n <= 16:
-        assert (host(ours) == O.ntt(host(x), u)).all()
+        assert (host(ours) == O.ntt(host(x), u, field)).all()

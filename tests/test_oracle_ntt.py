@@ -99,19 +99,24 @@ def test_roots_pq_omegas_distribute():
     assert got == [xs[i] * pw[((4 + i) % 12) % 3] % m for i in range(10)]
 
 
-@pytest.mark.skipif(not os.path.exists(REF_NTT), reason="reference NTT library not built")
-def test_pq_omegas_match_reference_host_code():
+REF_NTT_BLS = os.path.join(os.path.dirname(O.__file__), "_ref", "libref_ntt_bls12381_fr.so")
+
+
+@pytest.mark.parametrize("field,path", [(O.FR, REF_NTT), (O.BLS_FR, REF_NTT_BLS)])
+def test_pq_omegas_match_reference_host_code(field, path):
     """gen_pq_omegas is host code in the reference (precompute.cuh:100-125):
     run it from the reference's own library, no GPU involved."""
-    ref = ctypes.CDLL(REF_NTT)
+    if not os.path.exists(path):
+        pytest.skip("reference NTT library not built")
+    ref = ctypes.CDLL(path)
     ref.gen_pq_omegas.restype = None
     ref.gen_pq_omegas.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]
     for log_n, deg in ((12, 5), (20, 9), (3, 1), (24, 10)):
-        w = O.mont_limbs(O.root_of_unity(log_n))
+        w = O.mont_limbs(O.root_of_unity(log_n, field), field)
         pq = np.zeros(((1 << deg) >> 1 or 1, 8), np.uint32)
         om = np.zeros((32, 8), np.uint32)
         u = np.ascontiguousarray(w, dtype=np.uint32)
         ref.gen_pq_omegas(pq.ctypes.data, om.ctypes.data, deg, 1 << log_n, u.ctypes.data)
-        want_pq, want_om = O.pq_omegas(deg, 1 << log_n, w)
+        want_pq, want_om = O.pq_omegas(deg, 1 << log_n, w, field)
         assert (om == want_om).all(), (log_n, deg)
         assert (pq[: want_pq.shape[0]] == want_pq).all(), (log_n, deg)
