@@ -343,3 +343,25 @@ def test_reference_gpu_bls12381_default_config(M):
         assert (ref.msm(sc) == want).all()
     ref.close()
     ctx.close()
+
+
+@pytest.mark.skipif(not RG.available(16, 8, curve=RG.BLS12381), reason="reference GPU MSM (16, 8) for bls12381 not built")
+def test_reference_gpu_bls12381_tables_config(M):
+    # window 16 with 8 bucket sets: 16 signed-digit windows over two window tables
+    n = 1 << 17
+    d = M.gen_points_device(n, seed=34, curve=C)
+    h = M.to_host(d).reshape(n, PW)
+    ref = RG.RefGpuMsm(h, 16, 8, curve=RG.BLS12381)
+    assert ref.k == 2
+    tabs = ref.tables()
+    assert (tabs[:, :256] == O.precompute(h[:256], shift=16 * 8, n_tables=2, curve=C)).all()
+    # this library's drop-in in the same configuration, on the reference's tables
+    op = M.MSM(M.MsmConfig(window_size=16, target_window=8, curve=C))
+    buf, keep = M.alloc_gpu_buffer(op.get_buffer_size(n)[0])
+    for stream, dist in ((1, O.DIST_UNIFORM), (2, O.DIST_SKEWED)):
+        sc = O.gen_scalars(n, seed=34, stream=stream, dist=dist, curve=C)
+        want = O.msm(h, sc, curve=C)
+        assert (ref.msm(sc) == want).all(), dist
+        assert (op.run([tabs[0], tabs[1]], [sc], [buf])[0] == want).all(), dist
+    del keep
+    ref.close()
