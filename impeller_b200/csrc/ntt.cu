@@ -57,15 +57,18 @@ __device__ __forceinline__ u32 *at(const View &v, u64 i) {
     return v.base + 8 * p;
 }
 
+// Shared-memory tiles hold the two 16-byte halves of the elements in two
+// planes (half 0 of element e at s[e], half 1 at s[plane + e]): neighbouring
+// elements then sit in neighbouring 16-byte bank groups.
 template <class F>
-__device__ __forceinline__ void smem_store(uint4 *s, u32 e, const Fe<F> &a) {
-    s[2 * e] = make_uint4(a.l[0], a.l[1], a.l[2], a.l[3]);
-    s[2 * e + 1] = make_uint4(a.l[4], a.l[5], a.l[6], a.l[7]);
+__device__ __forceinline__ void smem_store(uint4 *s, u32 plane, u32 e, const Fe<F> &a) {
+    s[e] = make_uint4(a.l[0], a.l[1], a.l[2], a.l[3]);
+    s[plane + e] = make_uint4(a.l[4], a.l[5], a.l[6], a.l[7]);
 }
 
 template <class F>
-__device__ __forceinline__ Fe<F> smem_load(const uint4 *s, u32 e) {
-    const uint4 x = s[2 * e], y = s[2 * e + 1];
+__device__ __forceinline__ Fe<F> smem_load(const uint4 *s, u32 plane, u32 e) {
+    const uint4 x = s[e], y = s[plane + e];
     Fe<F> a;
     a.l[0] = x.x; a.l[1] = x.y; a.l[2] = x.z; a.l[3] = x.w;
     a.l[4] = y.x; a.l[5] = y.y; a.l[6] = y.z; a.l[7] = y.w;
@@ -93,7 +96,7 @@ __device__ __forceinline__ Fe<F> twiddle(const u32 *tw, u32 e) {
 // Stages go in pairs (s, s - 1); the two pairs of the lower stage share one
 // twiddle.  An odd last stage runs alone.  The sums of the first stage wait
 // in shared memory while its differences are multiplied, which keeps the
-// kernel at 76-78 registers: three 256-thread CTAs per SM (24 warps), 7.6 %
+// kernel at 76-80 registers: three 256-thread CTAs per SM (24 warps), 7.6 %
 // faster at 2^24 than holding all four values in registers (114 registers,
 // two CTAs).
 // rev_out (only when the tile is the whole array): write element p to
@@ -114,8 +117,8 @@ k_ntt_pass(View v, const u32 *tw, u32 L, u32 lo, u32 R, u32 logC, int rev_out) {
     for (u32 e = threadIdx.x; e < tsize; e += blockDim.x) {
         const u64 gi = gbase | ((u64)(e >> logC) << lo) | (e & (C - 1));
         const uint4 *p = reinterpret_cast<const uint4 *>(at(v, gi));
-        ntt_smem[2 * e] = p[0];
-        ntt_smem[2 * e + 1] = p[1];
+        ntt_smem[e] = p[0];
+        ntt_smem[tsize + e] = p[1];
     }
     __syncthreads();
 
@@ -137,28 +140,28 @@ k_ntt_pass(View v, const u32 *tw, u32 L, u32 lo, u32 R, u32 logC, int rev_out) {
             const u32 e0 = (d0 << logC) | c, eh = h << logC;
             Fe<F> b0, b1;
             {
-                const Fe<F> x0 = smem_load<F>(ntt_smem, e0), x2 = smem_load<F>(ntt_smem, e0 + 2 * eh);
+                const Fe<F> x0 = smem_load<F>(ntt_smem, tsize, e0), x2 = smem_load<F>(ntt_smem, tsize, e0 + 2 * eh);
                 b0 = fe_sub<F>(x0, x2);
-                smem_store<F>(ntt_smem, e0, fe_add<F>(x0, x2));  // a0, kept in place
+                smem_store<F>(ntt_smem, tsize, e0, fe_add<F>(x0, x2));  // a0, kept in place
             }
             if (ex0) b0 = fe_mul<F>(b0, twiddle<F, RECOMP>(tw, ex0));
             {
-                const Fe<F> x1 = smem_load<F>(ntt_smem, e0 + eh), x3 = smem_load<F>(ntt_smem, e0 + 3 * eh);
+                const Fe<F> x1 = smem_load<F>(ntt_smem, tsize, e0 + eh), x3 = smem_load<F>(ntt_smem, tsize, e0 + 3 * eh);
                 b1 = fe_sub<F>(x1, x3);
-                smem_store<F>(ntt_smem, e0 + eh, fe_add<F>(x1, x3));  // a1
+                smem_store<F>(ntt_smem, tsize, e0 + eh, fe_add<F>(x1, x3));  // a1
             }
             b1 = fe_mul<F>(b1, twiddle<F, RECOMP>(tw, ex1));  // ex1 != 0: bit (lo + sl - 1) of j is set
-            const Fe<F> a0 = smem_load<F>(ntt_smem, e0), a1 = smem_load<F>(ntt_smem, e0 + eh);
+            const Fe<F> a0 = smem_load<F>(ntt_smem, tsize, e0), a1 = smem_load<F>(ntt_smem, tsize, e0 + eh);
             Fe<F> y1 = fe_sub<F>(a0, a1), y3 = fe_sub<F>(b0, b1);
-            smem_store<F>(ntt_smem, e0, fe_add<F>(a0, a1));
-            smem_store<F>(ntt_smem, e0 + 2 * eh, fe_add<F>(b0, b1));
+            smem_store<F>(ntt_smem, tsize, e0, fe_add<F>(a0, a1));
+            smem_store<F>(ntt_smem, tsize, e0 + 2 * eh, fe_add<F>(b0, b1));
             if (ex2) {
                 const Fe<F> w2 = twiddle<F, RECOMP>(tw, ex2);
                 y1 = fe_mul<F>(y1, w2);
                 y3 = fe_mul<F>(y3, w2);
             }
-            smem_store<F>(ntt_smem, e0 + eh, y1);
-            smem_store<F>(ntt_smem, e0 + 3 * eh, y3);
+            smem_store<F>(ntt_smem, tsize, e0 + eh, y1);
+            smem_store<F>(ntt_smem, tsize, e0 + 3 * eh, y3);
         }
         __syncthreads();
         sl -= 2;
@@ -168,19 +171,19 @@ k_ntt_pass(View v, const u32 *tw, u32 L, u32 lo, u32 R, u32 logC, int rev_out) {
         for (u32 b = threadIdx.x; b < tsize / 2; b += blockDim.x) {
             const u32 c = b & (C - 1);
             const u32 e0 = ((b >> logC) << (logC + 1)) | c, e1 = e0 + C;
-            const Fe<F> x = smem_load<F>(ntt_smem, e0), y = smem_load<F>(ntt_smem, e1);
+            const Fe<F> x = smem_load<F>(ntt_smem, tsize, e0), y = smem_load<F>(ntt_smem, tsize, e1);
             Fe<F> dif = fe_sub<F>(x, y);
             const u32 ex = ((u32)(low0 + c)) << (L - 1 - s);
             if (ex) dif = fe_mul<F>(dif, twiddle<F, RECOMP>(tw, ex));
-            smem_store<F>(ntt_smem, e0, fe_add<F>(x, y));
-            smem_store<F>(ntt_smem, e1, dif);
+            smem_store<F>(ntt_smem, tsize, e0, fe_add<F>(x, y));
+            smem_store<F>(ntt_smem, tsize, e1, dif);
         }
         __syncthreads();
     }
 
     if (rev_out) {
         for (u32 e = threadIdx.x; e < tsize; e += blockDim.x) {
-            const Fe<F> a = fe_canon<F>(smem_load<F>(ntt_smem, e));
+            const Fe<F> a = fe_canon<F>(smem_load<F>(ntt_smem, tsize, e));
             fe_store(at(v, brev(e, L)), a);
         }
         return;
@@ -188,8 +191,8 @@ k_ntt_pass(View v, const u32 *tw, u32 L, u32 lo, u32 R, u32 logC, int rev_out) {
     for (u32 e = threadIdx.x; e < tsize; e += blockDim.x) {
         const u64 gi = gbase | ((u64)(e >> logC) << lo) | (e & (C - 1));
         uint4 *p = reinterpret_cast<uint4 *>(at(v, gi));
-        p[0] = ntt_smem[2 * e];
-        p[1] = ntt_smem[2 * e + 1];
+        p[0] = ntt_smem[e];
+        p[1] = ntt_smem[tsize + e];
     }
 }
 
@@ -209,20 +212,20 @@ __global__ void __launch_bounds__(256) k_ntt_reverse(View v, u32 L) {
     const u32 sh = L - REV_T;
     {
         const uint4 *p = reinterpret_cast<const uint4 *>(at(v, ((u64)a << sh) | ((u64)b << REV_T) | c));
-        tl[0][2 * (a * 17 + c)] = p[0];
-        tl[0][2 * (a * 17 + c) + 1] = p[1];
+        tl[0][a * 17 + c] = p[0];
+        tl[0][16 * 17 + a * 17 + c] = p[1];
         if (rb != b) {
             const uint4 *q = reinterpret_cast<const uint4 *>(at(v, ((u64)a << sh) | ((u64)rb << REV_T) | c));
-            tl[1][2 * (a * 17 + c)] = q[0];
-            tl[1][2 * (a * 17 + c) + 1] = q[1];
+            tl[1][a * 17 + c] = q[0];
+            tl[1][16 * 17 + a * 17 + c] = q[1];
         }
     }
     __syncthreads();
     // destination (a, rb, c) <- source (rev4(c), b, rev4(a)), and the mirror
     const u32 src = brev(c, REV_T) * 17 + brev(a, REV_T);
-    fe_store(at(v, ((u64)a << sh) | ((u64)rb << REV_T) | c), fe_canon<F>(smem_load<F>(tl[0], src)));
+    fe_store(at(v, ((u64)a << sh) | ((u64)rb << REV_T) | c), fe_canon<F>(smem_load<F>(tl[0], 16 * 17, src)));
     if (rb != b)
-        fe_store(at(v, ((u64)a << sh) | ((u64)b << REV_T) | c), fe_canon<F>(smem_load<F>(tl[1], src)));
+        fe_store(at(v, ((u64)a << sh) | ((u64)b << REV_T) | c), fe_canon<F>(smem_load<F>(tl[1], 16 * 17, src)));
 }
 
 // omegas[k] = u^(2^k), k < 33 (one thread).
