@@ -241,27 +241,12 @@ void dispatcher(impeller_server *s) {
 
 }  // namespace
 
-extern "C" {
-
-cudaError_t impeller_server_create(impeller_server **out, impeller_ctx *ctx, uint32_t max_batch,
-                                   uint32_t max_inflight, uint64_t hbm_budget) {
-    if (!out || !ctx || max_batch == 0 || max_inflight == 0 || max_inflight > 16) {
-        set_error("impeller_server_create: bad argument");
-        return cudaErrorInvalidValue;
-    }
-    std::unique_ptr<impeller_server> s(new impeller_server());
-    s->ctx = ctx;
-    s->max_batch = max_batch;
-    s->max_inflight = max_inflight;
-    cudaError_t e = cudaSetDevice(ctx->device);
-    if (e != cudaSuccess) return e;
-    if (hbm_budget == 0) {
-        size_t fr = 0, tot = 0;
-        if ((e = cudaMemGetInfo(&fr, &tot)) != cudaSuccess) return e;
-        const size_t reserve = (size_t)1 << 30;
-        hbm_budget = fr > reserve ? fr - reserve : fr / 2;
-    }
-    s->budget = hbm_budget;
+// Streams, pinned buffers and the scratch pool of a new server.
+static cudaError_t server_setup(impeller_server *s) {
+    cudaError_t e = cudaSuccess;
+    const impeller_ctx *ctx = s->ctx;
+    const u32 max_batch = s->max_batch, max_inflight = s->max_inflight;
+    const u64 hbm_budget = s->budget;
     {
         // a pool of its own that returns nothing to the driver between batches
         // (the default pool unmaps freed memory at every synchronisation,
@@ -302,6 +287,49 @@ cudaError_t impeller_server_create(impeller_server **out, impeller_ctx *ctx, uin
         if ((e = cudaMallocFromPoolAsync(&warm, reserve, s->pool, s->streams[0])) != cudaSuccess) return e;
         if ((e = cudaFreeAsync(warm, s->streams[0])) != cudaSuccess) return e;
         if ((e = cudaStreamSynchronize(s->streams[0])) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Frees what server_setup made (streams idle).
+static void server_release(impeller_server *s) {
+    for (auto st : s->streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    s->streams.clear();
+    for (auto p : s->pinned) cudaFreeHost(p);
+    s->pinned.clear();
+    for (auto p : s->staging) cudaFreeHost(p);
+    s->staging.clear();
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    s->pool = nullptr;
+}
+
+extern "C" {
+
+cudaError_t impeller_server_create(impeller_server **out, impeller_ctx *ctx, uint32_t max_batch,
+                                   uint32_t max_inflight, uint64_t hbm_budget) {
+    if (!out || !ctx || max_batch == 0 || max_inflight == 0 || max_inflight > 16) {
+        set_error("impeller_server_create: bad argument");
+        return cudaErrorInvalidValue;
+    }
+    std::unique_ptr<impeller_server> s(new impeller_server());
+    s->ctx = ctx;
+    s->max_batch = max_batch;
+    s->max_inflight = max_inflight;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return e;
+    if (hbm_budget == 0) {
+        size_t fr = 0, tot = 0;
+        if ((e = cudaMemGetInfo(&fr, &tot)) != cudaSuccess) return e;
+        const size_t reserve = (size_t)1 << 30;
+        hbm_budget = fr > reserve ? fr - reserve : fr / 2;
+    }
+    s->budget = hbm_budget;
+    if ((e = server_setup(s.get())) != cudaSuccess) {
+        server_release(s.get());
+        return e;
     }
     impeller_server *raw = s.release();
     raw->worker = std::thread(dispatcher, raw);
@@ -422,13 +450,7 @@ cudaError_t impeller_server_destroy(impeller_server *s) {
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->ctx->device);
-    for (auto st : s->streams) {
-        cudaStreamSynchronize(st);
-        cudaStreamDestroy(st);
-    }
-    for (auto p : s->pinned) cudaFreeHost(p);
-    for (auto p : s->staging) cudaFreeHost(p);
-    if (s->pool) cudaMemPoolDestroy(s->pool);
+    server_release(s);
     delete s;
     return cudaSuccess;
 }
