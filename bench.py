@@ -38,6 +38,11 @@ UNIT = "points/s"
 KERNELS_PER_MSM = 16
 
 
+def workload_name(log2n: int) -> str:
+    """The workload both arms time, by the same name."""
+    return f"plain single BN254 G1 MSM, n=2^{log2n}, P_i = r_i*G (seed 0), uniform Fr scalars"
+
+
 def env_int(name, default):
     try:
         return int(os.environ.get(name, default))
@@ -152,7 +157,7 @@ MULS_PER_MADD = 10
 
 # ------------------------------------------------------------- reference
 
-def reference_gpu(args, n: int, cores: int) -> dict:
+def reference_gpu(args, n: int, cores: int, pts: np.ndarray, scal: list) -> dict:
     """The reference's own GPU MSM (core/src/msm/src/msm.cu built unmodified
     for sm_100a) on the full n-point workload, driven through its msm() C ABI
     as its Rust operator drives it: pinned host points and scalars, one
@@ -171,8 +176,6 @@ def reference_gpu(args, n: int, cores: int) -> dict:
     if not all(RG.available(*cfg) for _, cfg, _ in configs):
         return {"unavailable": "reference sm_100a MSM libraries not built (reference sources absent at build time)"}
     from oracle import oracle as O
-    pts = O.gen_points(n, seed=0, threads=cores)
-    scal = [O.gen_scalars(n, seed=0, stream=1 + v, threads=cores) for v in range(2)]
     out = {"n": n, "api": "reference msm() C ABI (core/src/msm/src/msm.h:4-11), sm_100a build of its sources, "
                           "pinned host buffers, blocking, wall clock", "unit": UNIT}
     for name, (c, alpha), parts in configs:
@@ -181,7 +184,6 @@ def reference_gpu(args, n: int, cores: int) -> dict:
         out[name] = {"window_size": c, "target_window": alpha, "parts": parts, "n_precompute": ref.k,
                      "ms_per_call": ms, "value": n / (ms / 1e3)}
         ref.close()
-    del pts, scal
     if RG.available(16, 16, curve=RG.BLS12381):
         # the same call on the reference's second curve (its msm.cu built for bls12381)
         bp = O.gen_points(n, seed=0, threads=cores, curve=O.BLS12381)
@@ -197,33 +199,33 @@ def reference_gpu(args, n: int, cores: int) -> dict:
 def run_reference(args, rank, world):
     """--impl reference: the reference's CPU MSM (the C restatement of
     core/tests/msm_halo2.rs best_multiexp; the Rust original cannot be built
-    here) on the box's host cores, on bounded samples of the 2^22 workload.
-    The line also carries `reference_gpu`: the reference's own sm_100a MSM
-    kernel on the full workload on the same B200."""
+    here) on all of the box's host cores, one full 2^22-point MSM per step,
+    as the reference's own test times best_multiexp on the whole input
+    (core/tests/msm.rs:155-163).  The line also carries `reference_gpu`: the
+    reference's own sm_100a MSM kernel on the same workload on the same B200."""
     if rank != 0:
         return
     from oracle import oracle as O
     cores = os.cpu_count() or 1
     n_full = 1 << args.log2n
-    sample = min(n_full, 1 << 18)
-    gpu_leg = reference_gpu(args, n_full, cores)
-    pts = O.gen_points(sample, seed=0, threads=cores)
-    scal = [O.gen_scalars(sample, seed=0, stream=1 + v, threads=cores) for v in range(2)]
+    pts = O.gen_points(n_full, seed=0, threads=cores)
+    scal = [O.gen_scalars(n_full, seed=0, stream=1 + v, threads=cores) for v in range(2)]
+    gpu_leg = reference_gpu(args, n_full, cores, pts, scal)
     for w in range(args.warmup):
         O.msm(pts, scal[w % 2], threads=cores)
     t0 = time.perf_counter()
     for k in range(args.steps):
         O.msm(pts, scal[k % 2], threads=cores)
     dt = (time.perf_counter() - t0) / args.steps
-    value = sample / dt
+    value = n_full / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (254-bit Montgomery)", "data": "synthetic (seeded r_i*G, uniform Fr)",
-        "config": {"workload": f"BN254 G1 MSM, n=2^{args.log2n} (each step a 2^18-point prefix on the CPU)",
-                   "threads": cores},
+        "config": {"workload": workload_name(args.log2n), "n": n_full, "threads": cores,
+                   "cpu": "the whole input per step, all host threads"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"2^18-point prefix of the 2^{args.log2n} workload per step"},
+                         "sample": f"the full 2^{args.log2n}-point MSM per step (two alternating scalar vectors)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_gpu": gpu_leg,
         "reference_gpu_ntt": reference_gpu_ntt(args),
@@ -442,8 +444,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32 (254-bit Montgomery, 8x32-bit limbs)",
             "data": "synthetic: P_i = r_i*G (r_i uniform Fr, seed 0), uniform Fr scalars (seeded streams)",
-            "config": {"workload": f"plain single BN254 G1 MSM, n=2^{args.log2n}, window c={c} (autotune table)",
-                       "n": n, "window": c, "window_tables": bool(c_tab),
+            "config": {"workload": workload_name(args.log2n), "n": n, "window": c, "window_source": "autotune table",
+                       "window_tables": bool(c_tab),
                        "window_tables_setup_s": round(precompute_s, 3) if c_tab else None,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs > L2: 256 MiB points + 4 rotating 128 MiB scalar vectors"},

@@ -232,10 +232,18 @@ struct CardJob {
 
 // Plans persist per device across calls (their pinned table images and
 // events are the costly part to create); calls on one device are serialized.
+// Each call takes a new generation; a plan used by the current call carries
+// it and is never evicted, so a call may hold more plans than the cap.
+struct CachedPlan {
+    std::unique_ptr<Plan> plan;
+    u64 gen = 0;  // generation of the last call that used it
+};
+
 struct DevicePlans {
     std::mutex mu;
-    std::map<std::vector<u32>, std::unique_ptr<Plan>> plans;
+    std::map<std::vector<u32>, CachedPlan> plans;
     std::vector<std::vector<u32>> order;  // oldest first
+    u64 gen = 0;                          // current call
     void *host_images = nullptr;          // pinned: the chunk table images of one call
     size_t host_images_cap = 0;
 };
@@ -254,15 +262,24 @@ constexpr size_t PLAN_CACHE_CAP = 32;
 Plan *cached_plan(DevicePlans &D, int device, const Config &cfg, u32 M, u32 n, u32 stride) {
     std::vector<u32> key{cfg.c, cfg.n_windows, M, n, stride, cfg.curve};
     auto it = D.plans.find(key);
-    if (it != D.plans.end()) return it->second.get();
+    if (it != D.plans.end()) {
+        it->second.gen = D.gen;
+        return it->second.plan.get();
+    }
     if (D.plans.size() >= PLAN_CACHE_CAP) {
-        D.plans.erase(D.order.front());  // the oldest: not used by the current call
-        D.order.erase(D.order.begin());
+        // evict the oldest plan that the current call has not used
+        for (size_t k = 0; k < D.order.size(); k++) {
+            auto victim = D.plans.find(D.order[k]);
+            if (victim->second.gen == D.gen) continue;
+            D.plans.erase(victim);
+            D.order.erase(D.order.begin() + k);
+            break;
+        }
     }
     std::unique_ptr<Plan> p(new Plan());
     if (!Plan::build(*p, device, group_shapes(cfg, M, n, stride))) return nullptr;
     Plan *raw = p.get();
-    D.plans[key] = std::move(p);
+    D.plans[key] = CachedPlan{std::move(p), D.gen};
     D.order.push_back(key);
     return raw;
 }
@@ -272,6 +289,7 @@ cudaError_t run_card(CardJob &J) {
     CK(cudaSetDevice(J.device));
     DevicePlans &D = device_plans(J.device);
     std::lock_guard<std::mutex> hold(D.mu);
+    D.gen++;  // plans this call uses are pinned in the cache until the next call
     cudaStream_t st = device_stream(J.device, 0), cs = device_stream(J.device, 1);
     if (!st || !cs) {
         set_error("could not create a stream");

@@ -25,7 +25,9 @@
 //
 // Set-up: the first call on a device looks up the array's device address
 // with cudaGetSymbolAddress (with that device current) and caches it; make
-// that first call before any stream capture.  The kernels are the engine's
+// that first call before any stream capture.  The cached address outlives a
+// cudaDeviceReset, which releases the module the array lives in, so a reset
+// after the first call is not supported.  The kernels are the engine's
 // own (msm_kernels.cuh), compiled into this file under their own namespace.
 #include <cstdio>
 #include <mutex>

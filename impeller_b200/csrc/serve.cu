@@ -17,6 +17,7 @@
 // (scheduler/src/scheduler/core.rs:419-580, scheduler/src/scheduler.rs:432-489);
 // the admission-by-free-memory rule is the same idea applied per MSM, on HBM.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -241,6 +242,23 @@ void dispatcher(impeller_server *s) {
 
 }  // namespace
 
+// Test hook: the next server creation fails at this setup step (0: none).
+static std::atomic<u32> g_fail_setup_step{0};
+
+// Records which setup step failed and why; a step named by the test hook
+// fails with cudaErrorMemoryAllocation before it runs.
+static cudaError_t setup_step(const char *what, cudaError_t e) {
+    if (e != cudaSuccess) set_error(std::string("impeller_server_create: ") + what + ": " + cudaGetErrorString(e));
+    return e;
+}
+
+static cudaError_t injected(u32 step, const char *what) {
+    u32 want = step;
+    if (g_fail_setup_step.compare_exchange_strong(want, 0u))
+        return setup_step(what, cudaErrorMemoryAllocation);
+    return cudaSuccess;
+}
+
 // Streams, pinned buffers and the scratch pool of a new server.
 static cudaError_t server_setup(impeller_server *s) {
     cudaError_t e = cudaSuccess;
@@ -255,9 +273,11 @@ static cudaError_t server_setup(impeller_server *s) {
         props.allocType = cudaMemAllocationTypePinned;
         props.location.type = cudaMemLocationTypeDevice;
         props.location.id = ctx->device;
-        if ((e = cudaMemPoolCreate(&s->pool, &props)) != cudaSuccess) return e;
+        if ((e = injected(1, "memory pool")) != cudaSuccess) return e;
+        if ((e = setup_step("memory pool", cudaMemPoolCreate(&s->pool, &props))) != cudaSuccess) return e;
         uint64_t keep = hbm_budget;
-        if ((e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+        e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (setup_step("memory pool release threshold", e) != cudaSuccess) {
             cudaMemPoolDestroy(s->pool);
             s->pool = nullptr;
             return e;
@@ -265,16 +285,20 @@ static cudaError_t server_setup(impeller_server *s) {
     }
     for (u32 i = 0; i < max_inflight; i++) {
         cudaStream_t st;
-        if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = injected(2, "stream")) != cudaSuccess) return e;
+        if ((e = setup_step("stream", cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking))) != cudaSuccess)
+            return e;
         s->streams.push_back(st);
         u32 *p = nullptr;
-        if ((e = cudaHostAlloc(&p, (size_t)max_batch * point_words(ctx->curve) * 4, cudaHostAllocPortable)) !=
-            cudaSuccess)
-            return e;
+        if ((e = injected(3, "pinned result buffer")) != cudaSuccess) return e;
+        e = cudaHostAlloc(&p, (size_t)max_batch * point_words(ctx->curve) * 4, cudaHostAllocPortable);
+        if (setup_step("pinned result buffer", e) != cudaSuccess) return e;
         s->pinned.push_back(p);
         void *t = nullptr;
         s->staging_cap = (size_t)max_batch * 4096 + (1u << 20);  // descriptors, windows, reduce blocks
-        if ((e = cudaHostAlloc(&t, s->staging_cap, cudaHostAllocPortable)) != cudaSuccess) return e;
+        if ((e = setup_step("pinned staging buffer", cudaHostAlloc(&t, s->staging_cap, cudaHostAllocPortable))) !=
+            cudaSuccess)
+            return e;
         s->staging.push_back(t);
     }
     {
@@ -284,9 +308,11 @@ static cudaError_t server_setup(impeller_server *s) {
         // is freed (release threshold = budget), so this stays mapped.
         void *warm = nullptr;
         const size_t reserve = (size_t)std::min<u64>(s->budget, POOL_RESERVE);
-        if ((e = cudaMallocFromPoolAsync(&warm, reserve, s->pool, s->streams[0])) != cudaSuccess) return e;
-        if ((e = cudaFreeAsync(warm, s->streams[0])) != cudaSuccess) return e;
-        if ((e = cudaStreamSynchronize(s->streams[0])) != cudaSuccess) return e;
+        if ((e = injected(4, "pool reserve")) != cudaSuccess) return e;
+        e = cudaMallocFromPoolAsync(&warm, reserve, s->pool, s->streams[0]);
+        if (setup_step("pool reserve", e) != cudaSuccess) return e;
+        if ((e = setup_step("pool reserve release", cudaFreeAsync(warm, s->streams[0]))) != cudaSuccess) return e;
+        if ((e = setup_step("pool reserve sync", cudaStreamSynchronize(s->streams[0]))) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
@@ -318,11 +344,11 @@ cudaError_t impeller_server_create(impeller_server **out, impeller_ctx *ctx, uin
     s->ctx = ctx;
     s->max_batch = max_batch;
     s->max_inflight = max_inflight;
-    cudaError_t e = cudaSetDevice(ctx->device);
+    cudaError_t e = setup_step("cudaSetDevice", cudaSetDevice(ctx->device));
     if (e != cudaSuccess) return e;
     if (hbm_budget == 0) {
         size_t fr = 0, tot = 0;
-        if ((e = cudaMemGetInfo(&fr, &tot)) != cudaSuccess) return e;
+        if ((e = setup_step("cudaMemGetInfo", cudaMemGetInfo(&fr, &tot))) != cudaSuccess) return e;
         const size_t reserve = (size_t)1 << 30;
         hbm_budget = fr > reserve ? fr - reserve : fr / 2;
     }
@@ -377,6 +403,7 @@ static cudaError_t take_result(impeller_server *s, std::unordered_map<u64, Job>:
     if (h_result && st == cudaSuccess) std::memcpy(h_result, j.result, point_words(s->ctx->curve) * 4);
     if (latency_ms) *latency_ms = (j.t_done - j.t_submit) * 1e3;
     s->jobs.erase(it);
+    s->cv_done.notify_all();  // other waiters on this id find it gone
     if (st != cudaSuccess) set_error(std::string("MSM job failed: ") + cudaGetErrorString(st));
     return st;
 }
@@ -389,8 +416,18 @@ cudaError_t impeller_server_wait(impeller_server *s, uint64_t job_id, uint32_t *
         set_error("impeller_server_wait: unknown job");
         return cudaErrorInvalidValue;
     }
-    s->cv_done.wait(lk, [&] { return s->jobs[job_id].done; });
-    return take_result(s, s->jobs.find(job_id), h_result, latency_ms);
+    // Wake when the job is done, or gone: another wait() or poll() on the
+    // same id may take (and erase) it first.
+    s->cv_done.wait(lk, [&] {
+        auto j = s->jobs.find(job_id);
+        return j == s->jobs.end() || j->second.done;
+    });
+    it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) {
+        set_error("impeller_server_wait: job already taken by another wait or poll");
+        return cudaErrorInvalidValue;
+    }
+    return take_result(s, it, h_result, latency_ms);
 }
 
 cudaError_t impeller_server_poll(impeller_server *s, uint64_t job_id, uint32_t *h_result, double *latency_ms) {
@@ -431,6 +468,15 @@ cudaError_t impeller_server_get_stats(impeller_server *s, impeller_server_stats 
         for (double v : l) sum += v;
         out->mean_ms = sum / (double)l.size();
     }
+    return cudaSuccess;
+}
+
+cudaError_t impeller_server_fail_setup_step(uint32_t step) {
+    if (step > 4) {
+        set_error("impeller_server_fail_setup_step: steps are 1..4 (0 clears)");
+        return cudaErrorInvalidValue;
+    }
+    g_fail_setup_step.store(step);
     return cudaSuccess;
 }
 

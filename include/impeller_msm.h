@@ -209,7 +209,9 @@ cudaError_t impeller_server_create(impeller_server **out, impeller_ctx *ctx, uin
  * n > SRS length, NULL scalars (cudaErrorInvalidValue) and jobs whose device
  * footprint exceeds the budget (cudaErrorMemoryAllocation). */
 cudaError_t impeller_server_submit(impeller_server *s, const uint32_t *h_scalars, uint64_t n, uint64_t *job_id);
-/* Block until the job is done; copy its 16-word result; return its status. */
+/* Block until the job is done; copy its 16-word result; return its status.
+ * A job is taken once: a second wait (or poll) on the same id, concurrent or
+ * later, returns cudaErrorInvalidValue. */
 cudaError_t impeller_server_wait(impeller_server *s, uint64_t job_id, uint32_t *h_result, double *latency_ms);
 /* Like wait, but cudaErrorNotReady while the job is pending. */
 cudaError_t impeller_server_poll(impeller_server *s, uint64_t job_id, uint32_t *h_result, double *latency_ms);
@@ -217,6 +219,11 @@ cudaError_t impeller_server_get_stats(impeller_server *s, impeller_server_stats 
 /* Fail the next `batches` batches on the host, without GPU work (failure
  * handling tests: their jobs complete with cudaErrorLaunchFailure). */
 cudaError_t impeller_server_inject_failures(impeller_server *s, uint32_t batches);
+/* Test hook: the next impeller_server_create fails at setup step `step`
+ * (1 memory pool, 2 streams, 3 pinned buffers, 4 pool reserve; 0 clears)
+ * with cudaErrorMemoryAllocation, releasing what it had made; the message of
+ * impeller_last_error() names the step. */
+cudaError_t impeller_server_fail_setup_step(uint32_t step);
 /* Drain queued and running jobs, then stop. */
 cudaError_t impeller_server_destroy(impeller_server *s);
 
@@ -275,8 +282,11 @@ cudaError_t impeller_op_latency(int op, uint32_t iters, double *cycles_per_op);
  * the current device) and the output (d_result: 16 uint32, canonical affine).
  * n > IMPELLER_NOALLOC_MAX_N returns cudaErrorInvalidValue.  Every call shares
  * the one array, so calls that overlap on the GPU race: serialize them.  The
- * first call on a device looks up the array's address (cudaGetSymbolAddress);
- * make that first call before any stream capture.  Asynchronous on `stream`.
+ * first call on a device looks up the array's address (cudaGetSymbolAddress)
+ * and keeps it for the life of the process; make that first call before any
+ * stream capture.  A cudaDeviceReset after that first call is not supported:
+ * the kept address would refer to the released module.  Asynchronous on
+ * `stream`.
  */
 #define IMPELLER_NOALLOC_SCRATCH_BYTES (16u << 20)
 #define IMPELLER_NOALLOC_MAX_N (1u << 14)

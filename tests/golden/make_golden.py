@@ -4,6 +4,9 @@ the reference).
 
   python tests/golden/make_golden.py [REF_ROOT]
 
+REF_ROOT defaults to the REF_ROOT environment variable, else to a checkout
+named ``reference`` beside this repository.
+
 1. ``kat.json``: the reference's own known-answer vectors, parsed from its
    test sources (all values little-endian u32 limbs, as BIG_INTEGER_CHUNKS8
    stores them):
@@ -196,4 +199,5 @@ def bls_cases() -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    default_root = os.environ.get("REF_ROOT") or os.path.abspath(os.path.join(HERE, "..", "..", "..", "reference"))
+    main(sys.argv[1] if len(sys.argv) > 1 else default_root)

@@ -96,3 +96,53 @@ def test_injected_failure_then_recovery(M, srs):
     assert st["failed"] == 1 and st["completed"] == 1
     srv.close()
     ctx.close()
+
+
+def test_second_wait_on_a_taken_job_returns_an_error(M, srs):
+    # two threads wait on one job id: one takes the result, the other gets
+    # an error instead of blocking
+    import threading
+    ctx = M.MsmContext(srs[:2000])
+    srv = M.MsmServer(ctx, max_batch=4, max_inflight=1)
+    sc = O.gen_scalars(2000, seed=4, stream=4)
+    jid = srv.submit(sc)
+    outcomes = []
+
+    def waiter():
+        try:
+            outcomes.append(("ok", srv.wait(jid)[0]))
+        except M._lib.ImpellerError as e:
+            outcomes.append(("err", str(e)))
+
+    ts = [threading.Thread(target=waiter) for _ in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=60)
+    assert not any(t.is_alive() for t in ts)
+    oks = [o for o in outcomes if o[0] == "ok"]
+    errs = [o for o in outcomes if o[0] == "err"]
+    assert len(oks) == 1 and len(errs) == 1, outcomes
+    assert (oks[0][1] == O.msm(srs[:2000], sc)).all()
+    # and a later wait on the taken id is refused at once
+    with pytest.raises(M._lib.ImpellerError):
+        srv.wait(jid)
+    srv.close()
+    ctx.close()
+
+
+@pytest.mark.parametrize("step,what", [(1, "memory pool"), (2, "stream"), (3, "pinned result buffer"),
+                                       (4, "pool reserve")])
+def test_server_setup_failure_releases_and_recovers(M, srs, step, what):
+    # a failure injected on the host at each setup step: create returns the
+    # error with the step in the message, and a later create works
+    ctx = M.MsmContext(srs[:500])
+    L = M._lib.load()
+    M._lib.check(L.impeller_server_fail_setup_step(step), "fail_setup_step")
+    with pytest.raises(M._lib.ImpellerError, match=f"impeller_server_create: {what}: "):
+        M.MsmServer(ctx, max_batch=4, max_inflight=2, hbm_budget=64 << 20)
+    srv = M.MsmServer(ctx, max_batch=4, max_inflight=2, hbm_budget=64 << 20)
+    sc = O.gen_scalars(500, seed=5, stream=step)
+    assert (srv.wait(srv.submit(sc))[0] == O.msm(srs[:500], sc)).all()
+    srv.close()
+    ctx.close()

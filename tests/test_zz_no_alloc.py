@@ -4,14 +4,15 @@ impeller_msm_device_noalloc serves callers that cannot call cudaMalloc when
 they need an MSM (device memory planned ahead of time into a fixed arena,
 paths where an allocation would synchronize the device).  Its scratch is a
 static device array, so this test checks, through the C ABI, that two calls
-in a row give exactly the result of impeller_msm_device (bit-exact: integer
-work, tolerance zero), and that sizes beyond the array are refused.  This
-file is collected last so that a stop-at-first-failure run has already run
-every other test when it gets here; it also passes alone."""
-import ctypes
-
+in a row give exactly the result of impeller_msm_device and of the CPU
+oracle (bit-exact: integer work, tolerance zero), that an empty MSM gives
+the identity, and that sizes beyond the array are refused.  This file is
+collected last so that a stop-at-first-failure run has already run every
+other test when it gets here; it also passes alone."""
 import numpy as np
 import pytest
+
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -41,7 +42,19 @@ def test_noalloc_matches_allocating_entry_point_twice(M):
                      "impeller_msm_device_noalloc")
         torch.cuda.synchronize()
         assert torch.equal(got, want), f"call {call}: n={m}"
+        if m == 5000:
+            pts_h = M.to_host(pts).reshape(n, 16)[:m]
+            assert (M.to_host(got) == O.msm(pts_h, M.to_host(sc).reshape(m, 8))).all(), "oracle"
     ctx.close()
+
+
+def test_noalloc_empty_msm_is_identity(M):
+    L = M._lib.load()
+    out = torch.full((16,), -1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    M._lib.check(L.impeller_msm_device_noalloc(None, None, 0, out.data_ptr(), stream), "impeller_msm_device_noalloc")
+    torch.cuda.synchronize()
+    assert (M.to_host(out) == 0).all()
 
 
 def test_noalloc_rejects_oversize(M):
