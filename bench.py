@@ -31,11 +31,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "BN254 MSM points/s at 2^22; batched vs per-call speedup; p50/p99 latency"
 UNIT = "points/s"
-# kernels of one MSM run with the two-level sort: k_zero_words,
-# k_coarse_count, k_scan_reduce, k_scan_tiles, k_scan_down, k_coarse_scatter,
-# k_seg_plan, k_seg_hist, k_bin_scan, k_seg_scatter, k_accumulate,
-# k_fixup_short, k_fixup_long, k_reduce, k_window_sum, k_final
-KERNELS_PER_MSM = 16
 
 
 def workload_name(log2n: int) -> str:
@@ -449,7 +444,7 @@ def main():
                        "window_tables_setup_s": round(precompute_s, 3) if c_tab else None,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs > L2: 256 MiB points + 4 rotating 128 MiB scalar vectors"},
-            "gpu_launches": args.steps * KERNELS_PER_MSM,
+            "gpu_launches": args.steps * ctx.launches(n, c),
             "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
             "roofline": {"bound": "imad", "kernel": "k_accumulate", "achieved": achieved, "peak": peak.value,
                          "unit": "G 32x32->64 products/s", "frac": achieved / peak.value,
@@ -772,12 +767,13 @@ def batched_vs_per_call(M, ctx, dev, args) -> dict:
     tp = e[1].elapsed_time(e[2]) / reps
     same = bool(torch.equal(out, torch.stack(outs)))
     launches = b.launches
+    per_call_launches = sum(ctx.launches(s) for s in sizes)
     b.close()
     return {"workload": "64 MSMs, n log-uniform in [2^10, 2^20] (seed 0), prefixes of one resident SRS",
             "total_points": total, "batched_ms": tb, "per_call_ms": tp,
             "batched_points_per_s": total / (tb * 1e-3), "per_call_points_per_s": total / (tp * 1e-3),
             "speedup": tp / tb, "results_identical": same, "launches_per_batch": launches,
-            "launches_per_call_total": KERNELS_PER_MSM * len(sizes)}
+            "launches_per_call_total": per_call_launches}
 
 
 if __name__ == "__main__":

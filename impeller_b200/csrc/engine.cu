@@ -204,6 +204,40 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
         for (u32 k = 0; k < nblocks; k++) rblocks.push_back(make_uint2(wi, k));
         nparts += w.nparts;
     }
+    // reduction tree over the reduce warps' partials: levels of groups of
+    // 32, appended after the level-1 slots, until each window has one
+    std::vector<TreeGroup> groups;
+    p.tree_first.assign(1, 0);
+    {
+        const u32 nw = (u32)wins.size();
+        std::vector<u32> base(nw), count(nw), shift(nw);
+        std::vector<bool> done(nw, false);
+        for (u32 wi = 0; wi < nw; wi++) {
+            base[wi] = wins[wi].part_base;
+            count[wi] = wins[wi].nparts;
+            shift[wi] = 31 - __builtin_clz(wins[wi].chunk) + 5;
+        }
+        u32 left = nw;
+        while (left) {
+            for (u32 wi = 0; wi < nw; wi++) {
+                if (done[wi]) continue;
+                const u32 ng = (count[wi] + 31) / 32;
+                for (u32 g = 0; g < ng; g++)
+                    groups.push_back(TreeGroup{base[wi] + 32 * g, std::min(32u, count[wi] - 32 * g),
+                                               ng == 1 ? (TREE_FINAL | wi) : nparts + g, shift[wi]});
+                if (ng == 1) {
+                    done[wi] = true;
+                    left--;
+                } else {
+                    base[wi] = nparts;
+                    count[wi] = ng;
+                    shift[wi] += 5;
+                    nparts += ng;
+                }
+            }
+            p.tree_first.push_back((u32)groups.size());
+        }
+    }
     p.nparts = nparts;
     p.nwins = (u32)wins.size();
     p.nrblocks = (u32)rblocks.size();
@@ -245,12 +279,14 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     p.win_off = align_up(sizeof(MsmDesc) * p.M, 16);
     p.blk_off = p.win_off + align_up(sizeof(WinDesc) * wins.size(), 16);
     p.tf_off = p.blk_off + align_up(sizeof(uint2) * rblocks.size(), 16);
-    const size_t tbytes = align_up(p.tf_off + sizeof(u32) * (p.M + 1), 256);
+    p.tree_off = p.tf_off + align_up(sizeof(u32) * (p.M + 1), 16);
+    const size_t tbytes = align_up(p.tree_off + sizeof(TreeGroup) * groups.size(), 256);
     p.tables.assign(tbytes, 0);
     std::memcpy(p.tables.data() + p.desc_off, descs.data(), sizeof(MsmDesc) * p.M);
     std::memcpy(p.tables.data() + p.win_off, wins.data(), sizeof(WinDesc) * wins.size());
     std::memcpy(p.tables.data() + p.blk_off, rblocks.data(), sizeof(uint2) * rblocks.size());
     std::memcpy(p.tables.data() + p.tf_off, tile_first.data(), sizeof(u32) * (p.M + 1));
+    std::memcpy(p.tables.data() + p.tree_off, groups.data(), sizeof(TreeGroup) * groups.size());
 
     // device scratch layout
     PlanLayout &lo = p.layout;
@@ -299,7 +335,9 @@ Plan::~Plan() {
         for (auto e : set) cudaEventDestroy(e);
 }
 
-u32 Plan::launches() const { return msd ? 16 : 12; }
+// sort (10 kernels two-level, 6 per-entry) + accumulate, 2 fixups, reduce,
+// one per reduction-tree level, final
+u32 Plan::launches() const { return (msd ? 10u : 6u) + 5u + (u32)tree_first.size() - 1u; }
 
 const char *Plan::phase_name(int i) {
     static const char *names[NPHASE] = {"tables", "histogram", "scan", "scatter",
@@ -430,7 +468,7 @@ __global__ void k_zero_words(u32 *__restrict__ p, u32 n, u32 *__restrict__ q, u3
 // when d_image is given, so nothing here queues behind transfers on a copy
 // engine.
 cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, bool record_staged,
-                            const void *d_image) {
+                            const void *d_image, u32 *bucket_out) {
     const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, tf_off, scratch, nullptr, nullptr, d_image);
     cudaError_t pe;
     MARK(0);
@@ -504,13 +542,14 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
         MARK(4);
     }
 
-    AccumArgs aa{p.entries, p.offsets, nb, points, p.buckets, p.recb, p.recp};
+    u32 *const buckets = bucket_out ? bucket_out : p.buckets;
+    AccumArgs aa{p.entries, p.offsets, nb, points, buckets, p.recb, p.recp, bucket_out ? 1u : 0u};
     CURVE_LAUNCH(curve, k_accumulate, accum_blocks, accum_block, 0, st, aa);
     CK_LAUNCH("k_accumulate");
     MARK(5);
 
     const u32 T = accum_blocks * accum_block;
-    FixupArgs fa{p.offsets, nb, T, p.recb, p.recp, p.buckets, p.longl, long_cap};
+    FixupArgs fa{p.offsets, nb, T, p.recb, p.recp, buckets, p.longl, long_cap};
     CURVE_LAUNCH(curve, k_fixup_short, (T + 255) / 256, 256, 0, st, fa);
     CK_LAUNCH("k_fixup_short");
     CURVE_LAUNCH(curve, k_fixup_long, (u32)sm_count(device), 256, 0, st, fa);
@@ -530,9 +569,15 @@ cudaError_t Plan::run_tail(void *scratch, const u32 *buckets, bool dense, u32 *r
     CK_LAUNCH("k_reduce");
     MARK(7);
 
-    WindowSumArgs wa{p.desc, p.wins, p.parts, p.parts_s, nwins, p.wres};
-    CURVE_LAUNCH(curve, k_window_sum, nwins, WSUM_BLOCK, 0, st, wa);
-    CK_LAUNCH("k_window_sum");
+    const unsigned char *img = d_image ? static_cast<const unsigned char *>(d_image)
+                                       : static_cast<const unsigned char *>(scratch) + layout.o_tables;
+    const TreeGroup *groups = reinterpret_cast<const TreeGroup *>(img + tree_off);
+    for (size_t lv = 0; lv + 1 < tree_first.size(); lv++) {
+        const u32 cnt = tree_first[lv + 1] - tree_first[lv];
+        TreeArgs ta{groups + tree_first[lv], cnt, p.parts, p.parts_s, p.wres};
+        CURVE_LAUNCH(curve, k_reduce_tree, (cnt + TREE_WARPS - 1) / TREE_WARPS, TREE_BLOCK, 0, st, ta);
+        CK_LAUNCH("k_reduce_tree");
+    }
     FinalArgs fa2{p.desc, p.wres, M, carry_mode == 0 ? nullptr : p.carry, carry_mode == 2 ? 0 : 1, p.res};
     CURVE_LAUNCH(curve, k_final, (M + 31) / 32, 32, 0, st, fa2);
     CK_LAUNCH("k_final");
@@ -559,13 +604,18 @@ void Plan::write_image(void *dst, const u32 *const *scalars) const {
 
 cudaError_t Plan::launch_chunk(void *scratch, const u32 *points, u32 *acc, bool first, cudaStream_t st,
                                const void *d_image) {
-    cudaError_t e = run_front(scratch, points, st, true, d_image);
-    if (e != cudaSuccess) return e;
-    const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, tf_off, scratch, nullptr, nullptr, d_image);
-    const u32 blocks = std::max(1u, std::min((nb + 255) / 256, (u32)sm_count(device) * 8));
-    CURVE_LAUNCH(curve, k_bucket_merge, blocks, 256, 0, st, p.offsets, p.buckets, acc, nb, first ? 1u : 0u);
-    CK_LAUNCH("k_bucket_merge");
-    return cudaSuccess;
+    if (first) {
+        // every accumulator starts as the identity (all-zero XYZZ)
+        const u64 words = (u64)nb * xyzz_words(curve);
+        if (words >= (1ull << 32)) {
+            set_error("bucket accumulators exceed 2^32 words");
+            return cudaErrorInvalidValue;
+        }
+        k_zero_words<<<std::max(1u, std::min((u32)((words + 255) / 256), (u32)sm_count(device) * 8)), 256, 0, st>>>(
+            acc, (u32)words, nullptr, 0);
+        CK_LAUNCH("k_zero_words");
+    }
+    return run_front(scratch, points, st, true, d_image, acc);
 }
 
 cudaError_t Plan::launch_chunked_tail(void *scratch, const u32 *acc, u32 *results, int carry_mode, cudaStream_t st,
@@ -967,6 +1017,14 @@ cudaError_t impeller_ctx_profile_read(impeller_ctx *ctx, double *ms_per_phase, u
 }
 
 const char *impeller_phase_name(uint32_t i) { return Plan::phase_name((int)i); }
+
+uint32_t impeller_ctx_launches(impeller_ctx *ctx, uint64_t n, unsigned int c) {
+    if (!ctx || n == 0 || n > ctx->len) return 0;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (c == 0) c = ctx_window(ctx, n);
+    Plan *p = ctx_plan(ctx, (u32)n, c);
+    return p ? p->launches() : 0;
+}
 
 // ---------------------------------------------------------------- batches
 

@@ -97,8 +97,8 @@ class Plan {
 
     // Streamed accumulation, for points that arrive in chunks: each chunk
     // (this plan's MSMs over the chunk's points and scalars) sorts and
-    // accumulates, then adds its bucket sums into `acc` (nb XYZZ,
-    // caller-owned; first = overwrite).  launch_chunked_tail reduces `acc`
+    // accumulates its points straight into `acc` (nb XYZZ, caller-owned;
+    // first = set every bucket to the identity before).  launch_chunked_tail reduces `acc`
     // and emits results as launch does.  Every plan used on one `acc` must
     // have the same window structure (same c, windows and MSM count).
     // d_image: the chunk's table image (write_image) already on the device;
@@ -144,8 +144,10 @@ class Plan {
     Plan &operator=(const Plan &) = delete;
 
   private:
+    // bucket_out: accumulate into these buckets, each starting from its
+    // current value (streamed chunks); null = the plan's own buckets, fresh.
     cudaError_t run_front(void *scratch, const u32 *points, cudaStream_t stream, bool record_staged,
-                          const void *d_image);
+                          const void *d_image, u32 *bucket_out = nullptr);
     cudaError_t run_tail(void *scratch, const u32 *buckets, bool dense, u32 *results, int carry_mode,
                          cudaStream_t stream, u32 *carry_ext, const void *d_image);
 
@@ -154,8 +156,9 @@ class Plan {
     size_t ext_cap = 0;
     cudaEvent_t staged = nullptr;
     std::vector<unsigned char> tables;  // host image of the tables
-    size_t desc_off = 0, win_off = 0, blk_off = 0, tf_off = 0;
+    size_t desc_off = 0, win_off = 0, blk_off = 0, tf_off = 0, tree_off = 0;
     u32 nwins = 0, nrblocks = 0;
+    std::vector<u32> tree_first;  // reduction tree: first group of each level (+ total)
     bool profiling = false;
     std::vector<std::vector<cudaEvent_t>> prof_sets;  // one set of NPHASE+1 events per run
     u32 prof_used = 0;

@@ -529,6 +529,7 @@ struct AccumArgs {
     u32 *buckets;        // XYZZ, 32 u32 each, indexed by global bucket
     u32 *rec_bucket;     // 2 per thread
     u32 *rec_point;      // 2 per thread, XYZZ
+    u32 carry_in;        // 1: every bucket starts from its value in `buckets` (streamed chunks)
 };
 
 template <class C>
@@ -543,6 +544,10 @@ __device__ __forceinline__ AffineT<typename C::Fq> load_entry_point(const u32 *_
 // Otherwise the slice leaves a record: slot 2t for a piece that continues a
 // bucket begun in an earlier slice, slot 2t+1 for a piece whose bucket begins
 // in this slice and continues in later ones.
+// carry_in: the slice where a bucket begins starts it from the bucket's
+// current value in `buckets` (a streamed call adds every chunk's points into
+// accumulators that persist across its chunks; buckets without entries in
+// the chunk are left as they are).
 // One block of 384 threads per SM: 146 registers per thread with no spills,
 // 12 warps spread evenly over the SM's four schedulers.  Measured on B200 at
 // 2^22 this beats 2 x 256 threads at 128 registers (which spill) by 4%, and
@@ -588,7 +593,8 @@ __global__ void __launch_bounds__(ACCUM_THREADS, ACCUM_BLOCKS_PER_SM) k_accumula
         AffineT<FQ> q = nxt;
         if (pos + 1 < end) nxt = load_entry_point<C>(a.points, a.entries[pos + 1]);
         if (fresh) {
-            acc = xyzz_from_affine(q);
+            acc = (a.carry_in && bbeg >= start) ? xyzz_add_affine(xyzz_load<FQ>(a.buckets + (size_t)b * C::XW), q)
+                                                : xyzz_from_affine(q);
             fresh = false;
         } else {
             acc = xyzz_add_affine(acc, q);
@@ -667,26 +673,6 @@ __global__ void k_fixup_long(FixupArgs f) {
 #pragma unroll 1
         for (u32 o = 16; o; o >>= 1) acc = xyzz_add(acc, xyzz_shfl_down(acc, o));
         if (lane == 0) xyzz_store(f.buckets + (size_t)b * C::XW, acc);
-    }
-}
-
-// Streamed accumulation: an MSM whose points arrive in chunks runs the
-// sort and the accumulation per chunk and adds each chunk's bucket sums into
-// persistent accumulators `acc` (nb XYZZ); the reduction runs once, over
-// `acc` (dense).  first: acc = this chunk's sums (identity where empty).
-template <class C>
-__global__ void k_bucket_merge(const u32 *__restrict__ offsets, const u32 *__restrict__ buckets,
-                               u32 *__restrict__ acc, u32 nb, u32 first) {
-    using FQ = typename C::Fq;
-    constexpr u32 XW = C::XW;
-    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
-        const bool filled = offsets[g + 1] != offsets[g];
-        if (first) {
-            xyzz_store(acc + (size_t)g * XW, filled ? xyzz_load<FQ>(buckets + (size_t)g * XW) : xyzz_identity<FQ>());
-        } else if (filled) {
-            xyzz_store(acc + (size_t)g * XW,
-                       xyzz_add(xyzz_load<FQ>(acc + (size_t)g * XW), xyzz_load<FQ>(buckets + (size_t)g * XW)));
-        }
     }
 }
 
@@ -845,6 +831,73 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
             const u32 shift = ilog2(wd.chunk) + 5;  // 32 lanes per warp partial
             for (u32 k = 0; k < shift; k++) r2 = xyzz_dbl(r2);
             xyzz_store(a.wres + (size_t)win * C::XW, xyzz_add(v2, r2));
+        }
+    }
+}
+
+// ------------------------------------------------------ reduction tree
+//
+// After k_reduce, window total T = sum_g A_g + K * sum_g g * S_g over the
+// window's partials g (A = V, S of the reduce warps, K = 32 L).  One warp per
+// group of 32 consecutive partials g = 32 r + j folds them into one:
+//   A'_r = sum_j A_{32r+j} + K * sum_j j * S_{32r+j},   S'_r = sum_j S_{32r+j},
+// so that T = sum_r A'_r + 32 K * sum_r r * S'_r: the same form with K' = 32 K.
+// sum_j j * S_j = sum_{i >= 1} x_i for the inclusive suffix sums x of S.  A
+// window whose partials fit one group ends there: its total is A'_0.  Every
+// level is one launch over the groups of every window, so the tail runs on
+// many SMs instead of one block per window.
+
+struct TreeGroup {
+    u32 in_base;   // first input partial slot
+    u32 in_count;  // 1..32 partials
+    u32 out;       // output partial slot, or TREE_FINAL | window
+    u32 shift;     // log2 K of the input level
+};
+static constexpr u32 TREE_FINAL = 0x80000000u;
+static constexpr u32 TREE_BLOCK = 128;
+static constexpr u32 TREE_WARPS = TREE_BLOCK / 32;
+
+struct TreeArgs {
+    const TreeGroup *groups;  // this level's groups
+    u32 count;
+    u32 *parts_v;             // A per partial slot
+    u32 *parts_s;             // S per partial slot
+    u32 *wres;                // window totals
+};
+
+template <class C>
+__global__ void __launch_bounds__(TREE_BLOCK, C::XW == 32 ? 2 : 1) k_reduce_tree(TreeArgs a) {
+    using FQ = typename C::Fq;
+    using Xz = XyzzT<FQ>;
+    const u32 g = blockIdx.x * TREE_WARPS + (threadIdx.x >> 5);
+    if (g >= a.count) return;  // whole warps leave together
+    const u32 lane = threadIdx.x & 31u;
+    const TreeGroup gr = a.groups[g];
+    Xz A = xyzz_identity<FQ>(), x = xyzz_identity<FQ>();
+    if (lane < gr.in_count) {
+        A = xyzz_load<FQ>(a.parts_v + (size_t)(gr.in_base + lane) * C::XW);
+        x = xyzz_load<FQ>(a.parts_s + (size_t)(gr.in_base + lane) * C::XW);
+    }
+    // inclusive suffix sums of S
+#pragma unroll 1
+    for (u32 o = 1; o < 32; o <<= 1) {
+        Xz y = xyzz_shfl_down(x, o);
+        if (lane + o < 32) x = xyzz_add(x, y);
+    }
+    Xz w = lane ? x : xyzz_identity<FQ>();
+#pragma unroll 1
+    for (u32 o = 16; o; o >>= 1) {
+        A = xyzz_add(A, xyzz_shfl_down(A, o));
+        w = xyzz_add(w, xyzz_shfl_down(w, o));
+    }
+    if (lane == 0) {
+        for (u32 k = 0; k < gr.shift; k++) w = xyzz_dbl(w);
+        A = xyzz_add(A, w);
+        if (gr.out & TREE_FINAL) {
+            xyzz_store(a.wres + (size_t)(gr.out & ~TREE_FINAL) * C::XW, A);
+        } else {
+            xyzz_store(a.parts_v + (size_t)gr.out * C::XW, A);
+            xyzz_store(a.parts_s + (size_t)gr.out * C::XW, x);
         }
     }
 }

@@ -107,6 +107,7 @@ SIGNATURES: dict[str, tuple] = {
     "impeller_ctx_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_uint32,
                                                  ctypes.POINTER(ctypes.c_uint32)]),
     "impeller_phase_name": (ctypes.c_char_p, [ctypes.c_uint32]),
+    "impeller_ctx_launches": (ctypes.c_uint32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint]),
     "impeller_imad_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "impeller_imad_peak_curve": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint, ctypes.POINTER(ctypes.c_double)]),
     "impeller_op_latency": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),

@@ -357,6 +357,10 @@ class MsmContext:
     def window(self, n: int) -> int:
         return int(_lib.load().impeller_ctx_window(self.handle, n))
 
+    def launches(self, n: int, c: int = 0) -> int:
+        """Kernel launches of one MSM of n points with window c (0: the context's)."""
+        return int(_lib.load().impeller_ctx_launches(self.handle, n, c))
+
     def close(self) -> None:
         if self.handle:
             _lib.load().impeller_ctx_destroy(self.handle)

@@ -158,6 +158,9 @@ cudaError_t impeller_msm_host(impeller_ctx *ctx, const uint32_t *h_scalars, uint
 cudaError_t impeller_ctx_profile(impeller_ctx *ctx, int enable);
 cudaError_t impeller_ctx_profile_read(impeller_ctx *ctx, double *ms_per_phase, uint32_t nphase, uint32_t *runs);
 const char *impeller_phase_name(uint32_t i);
+/* Kernel launches of one MSM of n points with window c (0: the context's
+ * choice) on this context; 0 for invalid arguments. */
+uint32_t impeller_ctx_launches(impeller_ctx *ctx, uint64_t n, unsigned int c);
 
 /* ------------------------------------------------------------------------
  * Batched MSMs of uneven sizes over prefixes of the resident points: one
