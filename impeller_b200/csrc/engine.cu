@@ -243,11 +243,13 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     p.nrblocks = (u32)rblocks.size();
 
     // accumulate: persistent threads (every resident slot), at least 8 entries each
-    const u32 full_blocks = (u32)sms * ACCUM_PER_SM;
+    const bool bls = p.curve == CURVE_BLS12381;
+    const u32 accum_threads = bls ? AccumShape<Bls12381>::threads : AccumShape<Bn254>::threads;
+    const u32 full_blocks = (u32)sms * (bls ? AccumShape<Bls12381>::per_sm : AccumShape<Bn254>::per_sm);
     const u64 want_threads = (entries + 7) / 8;
     p.accum_blocks =
-        (u32)std::max<u64>(1, std::min<u64>(full_blocks, (want_threads + ACCUM_BLOCK - 1) / ACCUM_BLOCK));
-    p.accum_block = ACCUM_BLOCK;
+        (u32)std::max<u64>(1, std::min<u64>(full_blocks, (want_threads + accum_threads - 1) / accum_threads));
+    p.accum_block = accum_threads;
     const u32 T = p.accum_blocks * p.accum_block;
     p.long_cap = T;
     p.hist_grid_x = (u32)std::max<u64>(1, std::min<u64>((u64)sms * 8, (nmax + 255) / 256));

@@ -558,11 +558,21 @@ __device__ __forceinline__ AffineT<typename C::Fq> load_entry_point(const u32 *_
 #ifndef ACCUM_BLOCKS_PER_SM
 #define ACCUM_BLOCKS_PER_SM 1
 #endif
-static constexpr u32 ACCUM_BLOCK = ACCUM_THREADS;
-static constexpr u32 ACCUM_PER_SM = ACCUM_BLOCKS_PER_SM;
+// BLS12-381 (48-word XYZZ, 12-limb products) has its own block shape.
+#ifndef ACCUM_THREADS_BLS
+#define ACCUM_THREADS_BLS 384
+#endif
+#ifndef ACCUM_BLOCKS_PER_SM_BLS
+#define ACCUM_BLOCKS_PER_SM_BLS 1
+#endif
+template <class C>
+struct AccumShape {
+    static constexpr u32 threads = C::XW == 32 ? ACCUM_THREADS : ACCUM_THREADS_BLS;
+    static constexpr u32 per_sm = C::XW == 32 ? ACCUM_BLOCKS_PER_SM : ACCUM_BLOCKS_PER_SM_BLS;
+};
 
 template <class C>
-__global__ void __launch_bounds__(ACCUM_THREADS, ACCUM_BLOCKS_PER_SM) k_accumulate(AccumArgs a) {
+__global__ void __launch_bounds__(AccumShape<C>::threads, AccumShape<C>::per_sm) k_accumulate(AccumArgs a) {
     using FQ = typename C::Fq;
     const u32 T = gridDim.x * blockDim.x;
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
