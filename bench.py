@@ -454,12 +454,15 @@ def main():
                          "per_launch": {"madds": madds, "products_per_madd": MULS_PER_MADD * PRODUCTS_PER_MUL,
                                         "ms": acc_ms},
                          "peak_source": "impeller_imad_peak: independent Fq Montgomery products (4 chains/thread, 136 partial products each), measured live"},
-            "roofline_sort": {"bound": "hbm", "kernels": "k_histogram+k_scan+k_scatter",
-                              "achieved": sort_bytes / (sort_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                              "frac": sort_bytes / (sort_ms * 1e-3) / 1e9 / hbm_peak,
-                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
             "clocks": clocks,
         }
+        # the decompose + sort phase, bound by HBM: reported inside `roofline`
+        # so that it stays beside the headline kernel's figures
+        line["roofline"]["sort"] = {
+            "bound": "hbm", "kernels": "sort phase (every kernel from the scalar read to the bucket-ordered entries)",
+            "ms": sort_ms, "algorithmic_bytes": sort_bytes, "achieved": sort_bytes / (sort_ms * 1e-3) / 1e9,
+            "peak": hbm_peak, "unit": "GB/s", "frac": sort_bytes / (sort_ms * 1e-3) / 1e9 / hbm_peak,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
 
     legs = set(args.only.split(",")) if args.only else {"e2e", "resident", "batched", "served", "cpu", "bls12381",
                                                          "ntt"}
@@ -769,11 +772,27 @@ def batched_vs_per_call(M, ctx, dev, args) -> dict:
     launches = b.launches
     per_call_launches = sum(ctx.launches(s) for s in sizes)
     b.close()
+    # the same plan launched kernel by kernel from the host, without the graph:
+    # how much of the batched time the graph's launch savings account for
+    b2 = ctx.batch(sizes, graph=False)
+    out2 = torch.empty_like(out)
+    for _ in range(2):
+        b2.run(scal, out=out2)
+    torch.cuda.synchronize()
+    e[2].record(st)
+    for _ in range(reps):
+        b2.run(scal, out=out2)
+    e[3].record(st)
+    torch.cuda.synchronize()
+    tng = e[2].elapsed_time(e[3]) / reps
+    same = same and bool(torch.equal(out2, out))
+    b2.close()
     return {"workload": "64 MSMs, n log-uniform in [2^10, 2^20] (seed 0), prefixes of one resident SRS",
             "total_points": total, "batched_ms": tb, "per_call_ms": tp,
             "batched_points_per_s": total / (tb * 1e-3), "per_call_points_per_s": total / (tp * 1e-3),
             "speedup": tp / tb, "results_identical": same, "launches_per_batch": launches,
-            "launches_per_call_total": per_call_launches}
+            "launches_per_call_total": per_call_launches, "batched_no_graph_ms": tng,
+            "graph_saving_ms": tng - tb}
 
 
 if __name__ == "__main__":

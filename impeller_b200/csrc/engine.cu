@@ -506,7 +506,7 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
         k_scan_down<<<cscan_tiles, SCAN_BLOCK, 0, st>>>(cnt, ctiles, coff, ccur, ncnt, cscan_tiles);
         CK_LAUNCH("k_scan_down");
         MARK(3);
-        const size_t scatter_smem = ((size_t)2 * nbins + 2 * STAGE_ENTRIES) * 4;
+        const size_t scatter_smem = (size_t)2 * nbins * 4 + (size_t)STAGE_ENTRIES * 6;
         CK(sort_smem(device, curve, 0, scatter_smem));
         CURVE_LAUNCH(curve, k_coarse_scatter, sort_tiles, SORT_BLOCK, scatter_smem, st, sa);
         CK_LAUNCH("k_coarse_scatter");

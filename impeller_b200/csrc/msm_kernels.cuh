@@ -276,30 +276,36 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
     for (u32 b = threadIdx.x; b < a.nbins; b += blockDim.x) a.cnt[(size_t)b * a.ntiles + blockIdx.x] = hist[b];
 }
 
-// Shared memory: delta[nbins], cur[nbins], stage_e[STAGE_ENTRIES],
-// stage_f[STAGE_ENTRIES].  A tile holds at most STAGE_ENTRIES entries (the
-// plan sizes tiles by the largest window count).
+// Shared memory: delta[nbins], cur[nbins], stage_e[STAGE_ENTRIES] (u32),
+// stage_f[STAGE_ENTRIES] (u16: bucket within the bin).  A tile holds at most
+// STAGE_ENTRIES entries (the plan sizes tiles by the largest window count).
+// 6 staged bytes per entry keep two CTAs on an SM for plans of up to 2048
+// bins.  Only the bins of the tile's MSM are touched: a batch's other MSMs
+// own other bins.
 template <class C>
-__global__ void __launch_bounds__(SORT_BLOCK) k_coarse_scatter(SortArgs a) {
+__global__ void __launch_bounds__(SORT_BLOCK, 2) k_coarse_scatter(SortArgs a) {
     extern __shared__ u32 sm[];
     __shared__ u32 warp_tot[32];
-    u32 *delta = sm, *cur = sm + a.nbins, *stage_e = sm + 2 * a.nbins, *stage_f = stage_e + STAGE_ENTRIES;
+    u32 *delta = sm, *cur = sm + a.nbins, *stage_e = sm + 2 * a.nbins;
+    unsigned short *stage_f = reinterpret_cast<unsigned short *>(stage_e + STAGE_ENTRIES);
     const u32 tile = blockIdx.x;
     u32 m, start, end;
     sort_tile(a, tile, m, start, end);
     const MsmDesc d = a.descs[m];
+    const u32 B = 1u << (d.c - 1);
+    const u32 blo = d.bucket_base >> FINE_BITS, bhi = (d.bucket_base + d.n_windows * B - 1u) >> FINE_BITS;
     // this tile's bins: local start (exclusive scan of its counts) and the
     // distance from a local slot to the global coarse position
-    const u32 per = (a.nbins + blockDim.x - 1) / blockDim.x;
-    const u32 b0 = threadIdx.x * per;
+    const u32 per = (bhi - blo + blockDim.x) / blockDim.x;
+    const u32 b0 = blo + threadIdx.x * per;
     u32 sum = 0;
     for (u32 k = 0; k < per; k++)
-        if (b0 + k < a.nbins) sum += a.cnt[(size_t)(b0 + k) * a.ntiles + tile];
+        if (b0 + k <= bhi) sum += a.cnt[(size_t)(b0 + k) * a.ntiles + tile];
     u32 total;
     u32 run = block_scan_excl(sum, total, warp_tot);
     for (u32 k = 0; k < per; k++) {
         const u32 b = b0 + k;
-        if (b < a.nbins) {
+        if (b <= bhi) {
             const size_t ci = (size_t)b * a.ntiles + tile;
             cur[b] = run;
             delta[b] = a.coff[ci] - run;
@@ -307,7 +313,6 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_scatter(SortArgs a) {
         }
     }
     __syncthreads();
-    const u32 B = 1u << (d.c - 1);
     for (u32 base = start; base < end; base += blockDim.x) {
         const u32 i = base + threadIdx.x;
         const bool live = i < end;
@@ -321,20 +326,24 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_scatter(SortArgs a) {
             it.next(w, d.n_logical, mag, sign);
             if (mag) {
                 const u32 key = d.bucket_base + (w % d.n_windows) * B + mag - 1;
-                const u32 bin = key >> FINE_BITS;
-                const u32 slot = atomicAdd(&cur[bin], 1u);
+                const u32 slot = atomicAdd(&cur[key >> FINE_BITS], 1u);
                 const u32 table = w / d.n_windows;
                 stage_e[slot] = ((d.table_base + table * d.table_stride + i) << 1) | sign;
-                stage_f[slot] = (key & (FINE - 1u)) | (bin << 16);
+                stage_f[slot] = (unsigned short)(key & (FINE - 1u));
             }
         }
     }
     __syncthreads();
-    for (u32 s = threadIdx.x; s < total; s += blockDim.x) {
-        const u32 f = stage_f[s];
-        const u32 pos = delta[f >> 16] + s;
-        a.c_entry[pos] = stage_e[s];
-        a.c_fine[pos] = (unsigned short)(f & 0xffffu);
+    // one warp per bin writes the bin's run of this tile: one coalesced run
+    // of entries and one of bucket indices
+    const u32 lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
+    for (u32 b = blo + (threadIdx.x >> 5); b <= bhi; b += nw) {
+        const u32 s0 = b == blo ? 0u : cur[b - 1], s1 = cur[b];
+        const u32 g = delta[b];
+        for (u32 s = s0 + lane; s < s1; s += 32) {
+            a.c_entry[g + s] = stage_e[s];
+            a.c_fine[g + s] = stage_f[s];
+        }
     }
 }
 
@@ -367,13 +376,42 @@ __global__ void __launch_bounds__(FINE_BLOCK) k_seg_plan(SortArgs a) {
     if (threadIdx.x == 0) a.nsegs[0] = total;
 }
 
+// Entries of a segment are read 8 bucket indices (16 bytes) at a time, four
+// loads in flight per thread, so that the load latency overlaps.
+__device__ __forceinline__ void hist8(u32 *hist, uint4 q) {
+    atomicAdd(&hist[q.x & 0xffffu], 1u);
+    atomicAdd(&hist[q.x >> 16], 1u);
+    atomicAdd(&hist[q.y & 0xffffu], 1u);
+    atomicAdd(&hist[q.y >> 16], 1u);
+    atomicAdd(&hist[q.z & 0xffffu], 1u);
+    atomicAdd(&hist[q.z >> 16], 1u);
+    atomicAdd(&hist[q.w & 0xffffu], 1u);
+    atomicAdd(&hist[q.w >> 16], 1u);
+}
+
 __global__ void __launch_bounds__(FINE_BLOCK) k_seg_hist(SortArgs a) {
     __shared__ u32 hist[FINE];
     if (blockIdx.x >= a.nsegs[0]) return;
     const uint4 sg = a.segs[blockIdx.x];
     for (u32 f = threadIdx.x; f < FINE; f += blockDim.x) hist[f] = 0;
     __syncthreads();
-    for (u32 i = sg.y + threadIdx.x; i < sg.z; i += blockDim.x) atomicAdd(&hist[a.c_fine[i]], 1u);
+    // [y, v0) and [v1, z) one by one, [v0, v1) in aligned groups of 8
+    const u32 y = sg.y, z = sg.z;
+    const u32 v0 = min((y + 7u) & ~7u, z), v1 = v0 + ((z - v0) & ~7u);
+    const unsigned short *cf = a.c_fine;
+    if (threadIdx.x < v0 - y) atomicAdd(&hist[cf[y + threadIdx.x]], 1u);
+    if (threadIdx.x < z - v1) atomicAdd(&hist[cf[v1 + threadIdx.x]], 1u);
+    const uint4 *v = reinterpret_cast<const uint4 *>(cf + v0);
+    const u32 nv = (v1 - v0) >> 3, bd = blockDim.x;
+    u32 k = threadIdx.x;
+    for (; k + 3 * bd < nv; k += 4 * bd) {
+        const uint4 q0 = __ldg(v + k), q1 = __ldg(v + k + bd), q2 = __ldg(v + k + 2 * bd), q3 = __ldg(v + k + 3 * bd);
+        hist8(hist, q0);
+        hist8(hist, q1);
+        hist8(hist, q2);
+        hist8(hist, q3);
+    }
+    for (; k < nv; k += bd) hist8(hist, __ldg(v + k));
     __syncthreads();
     for (u32 f = threadIdx.x; f < FINE; f += blockDim.x) a.seghist[(size_t)blockIdx.x * FINE + f] = hist[f];
 }
@@ -407,7 +445,21 @@ __global__ void __launch_bounds__(FINE_BLOCK) k_bin_scan(SortArgs a) {
 }
 
 // Shared memory: lcur[FINE], delta[FINE], stage_e[SEG_ENTRIES],
-// stage_f[SEG_ENTRIES] (16-bit).
+// stage_f[SEG_ENTRIES] (16-bit).  Entries are read four at a time (16 bytes
+// of entries, 8 of bucket indices), two groups in flight per thread.
+__device__ __forceinline__ void place1(u32 *lcur, u32 *stage_e, unsigned short *stage_f, u32 fi, u32 e) {
+    const u32 slot = atomicAdd(&lcur[fi], 1u);
+    stage_e[slot] = e;
+    stage_f[slot] = (unsigned short)fi;
+}
+
+__device__ __forceinline__ void place4(u32 *lcur, u32 *stage_e, unsigned short *stage_f, uint2 f, uint4 e) {
+    place1(lcur, stage_e, stage_f, f.x & 0xffffu, e.x);
+    place1(lcur, stage_e, stage_f, f.x >> 16, e.y);
+    place1(lcur, stage_e, stage_f, f.y & 0xffffu, e.z);
+    place1(lcur, stage_e, stage_f, f.y >> 16, e.w);
+}
+
 __global__ void __launch_bounds__(FINE_BLOCK) k_seg_scatter(SortArgs a) {
     extern __shared__ u32 sm[];
     __shared__ u32 warp_tot[32];
@@ -423,12 +475,22 @@ __global__ void __launch_bounds__(FINE_BLOCK) k_seg_scatter(SortArgs a) {
     lcur[f] = ls;
     delta[f] = a.segcur[h + f] - ls;
     __syncthreads();
-    for (u32 i = sg.y + threadIdx.x; i < sg.z; i += blockDim.x) {
-        const u32 fi = a.c_fine[i];
-        const u32 slot = atomicAdd(&lcur[fi], 1u);
-        stage_e[slot] = a.c_entry[i];
-        stage_f[slot] = (unsigned short)fi;
+    // [y, v0) and [v1, z) one by one, [v0, v1) in aligned groups of 4
+    const u32 y = sg.y, z = sg.z;
+    const u32 v0 = min((y + 3u) & ~3u, z), v1 = v0 + ((z - v0) & ~3u);
+    if (threadIdx.x < v0 - y) place1(lcur, stage_e, stage_f, a.c_fine[y + threadIdx.x], a.c_entry[y + threadIdx.x]);
+    if (threadIdx.x < z - v1) place1(lcur, stage_e, stage_f, a.c_fine[v1 + threadIdx.x], a.c_entry[v1 + threadIdx.x]);
+    const uint2 *vf = reinterpret_cast<const uint2 *>(a.c_fine + v0);
+    const uint4 *ve = reinterpret_cast<const uint4 *>(a.c_entry + v0);
+    const u32 nv = (v1 - v0) >> 2, bd = blockDim.x;
+    u32 k = threadIdx.x;
+    for (; k + bd < nv; k += 2 * bd) {
+        const uint2 f0 = __ldg(vf + k), f1 = __ldg(vf + k + bd);
+        const uint4 e0 = __ldg(ve + k), e1 = __ldg(ve + k + bd);
+        place4(lcur, stage_e, stage_f, f0, e0);
+        place4(lcur, stage_e, stage_f, f1, e1);
     }
+    for (; k < nv; k += bd) place4(lcur, stage_e, stage_f, __ldg(vf + k), __ldg(ve + k));
     __syncthreads();
     for (u32 s = threadIdx.x; s < total; s += blockDim.x) a.entries[delta[stage_f[s]] + s] = stage_e[s];
 }
