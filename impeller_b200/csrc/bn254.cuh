@@ -431,6 +431,25 @@ __device__ __forceinline__ Fe<F> fe_sqr(const Fe<F> &a) {
     return fe_mul<F>(a, a);
 }
 
+// One out-of-line copy of the product, for kernels that run only a few warps
+// (the reduction tree, the final Horner and affine conversion): no other warp
+// reuses their instruction cache, and an inlined point addition (about 4000
+// instructions) streams through it, so a lone warp stalls on instruction
+// fetch.  The point formulas below take the product as a policy.
+template <class F>
+__device__ __noinline__ Fe<F> fe_mul_call(Fe<F> a, Fe<F> b) {
+    return fe_mul_inline<F>(a, b);
+}
+
+struct MulInline {
+    template <class F>
+    __device__ __forceinline__ static Fe<F> mul(const Fe<F> &a, const Fe<F> &b) { return fe_mul<F>(a, b); }
+};
+struct MulCall {
+    template <class F>
+    __device__ __forceinline__ static Fe<F> mul(const Fe<F> &a, const Fe<F> &b) { return fe_mul_call<F>(a, b); }
+};
+
 // Leave Montgomery form: a * R^{-1} mod N, canonical, for a in [0, 2N)
 // (Montgomery reduction only; the sum stays at or below N before the final
 // subtraction).
@@ -843,20 +862,20 @@ __device__ __forceinline__ XyzzT<F> affine_dbl(const AffineT<F> &a) {
 }
 
 // dbl-2008-s-1 with a = 0.
-template <class F>
+template <class F, class MUL = MulInline>
 __device__ __forceinline__ XyzzT<F> xyzz_dbl(const XyzzT<F> &p) {
     if (xyzz_is_identity(p)) return p;
     Fe<F> u = fe_dbl(p.y);
-    Fe<F> v = fe_sqr(u);
-    Fe<F> w = fe_mul(u, v);
-    Fe<F> s = fe_mul(p.x, v);
-    Fe<F> x2 = fe_sqr(p.x);
+    Fe<F> v = MUL::mul(u, u);
+    Fe<F> w = MUL::mul(u, v);
+    Fe<F> s = MUL::mul(p.x, v);
+    Fe<F> x2 = MUL::mul(p.x, p.x);
     Fe<F> m = fe_add(fe_dbl(x2), x2);
     XyzzT<F> r;
-    r.x = fe_sub(fe_sub(fe_sqr(m), s), s);
-    r.y = fe_sub(fe_mul(m, fe_sub(s, r.x)), fe_mul(w, p.y));
-    r.zz = fe_mul(v, p.zz);
-    r.zzz = fe_mul(w, p.zzz);
+    r.x = fe_sub(fe_sub(MUL::mul(m, m), s), s);
+    r.y = fe_sub(MUL::mul(m, fe_sub(s, r.x)), MUL::mul(w, p.y));
+    r.zz = MUL::mul(v, p.zz);
+    r.zzz = MUL::mul(w, p.zzz);
     return r;
 }
 
@@ -886,29 +905,29 @@ __device__ __forceinline__ XyzzT<F> xyzz_add_affine(const XyzzT<F> &p, const Aff
 }
 
 // add-2008-s: p + q.  Handles every special case.
-template <class F>
+template <class F, class MUL = MulInline>
 __device__ __forceinline__ XyzzT<F> xyzz_add(const XyzzT<F> &p, const XyzzT<F> &q) {
     if (xyzz_is_identity(p)) return q;
     if (xyzz_is_identity(q)) return p;
-    Fe<F> u1 = fe_mul(p.x, q.zz);
-    Fe<F> u2 = fe_mul(q.x, p.zz);
-    Fe<F> s1 = fe_mul(p.y, q.zzz);
-    Fe<F> s2 = fe_mul(q.y, p.zzz);
+    Fe<F> u1 = MUL::mul(p.x, q.zz);
+    Fe<F> u2 = MUL::mul(q.x, p.zz);
+    Fe<F> s1 = MUL::mul(p.y, q.zzz);
+    Fe<F> s2 = MUL::mul(q.y, p.zzz);
     Fe<F> P = fe_sub(u2, u1);
     Fe<F> R = fe_sub(s2, s1);
     if (fe_is_zero(P)) {
-        if (fe_is_zero(R)) return xyzz_dbl(p);
+        if (fe_is_zero(R)) return xyzz_dbl<F, MUL>(p);
         return xyzz_identity<F>();
     }
-    Fe<F> pp = fe_sqr(P);
-    Fe<F> ppp = fe_mul(P, pp);
-    Fe<F> Q = fe_mul(u1, pp);
+    Fe<F> pp = MUL::mul(P, P);
+    Fe<F> ppp = MUL::mul(P, pp);
+    Fe<F> Q = MUL::mul(u1, pp);
     XyzzT<F> r;
-    r.zz = fe_mul(fe_mul(p.zz, q.zz), pp);
-    r.zzz = fe_mul(fe_mul(p.zzz, q.zzz), ppp);
-    Fe<F> t = fe_mul(s1, ppp);
-    r.x = fe_sub(fe_sub(fe_sub(fe_sqr(R), ppp), Q), Q);
-    r.y = fe_sub(fe_mul(R, fe_sub(Q, r.x)), t);
+    r.zz = MUL::mul(MUL::mul(p.zz, q.zz), pp);
+    r.zzz = MUL::mul(MUL::mul(p.zzz, q.zzz), ppp);
+    Fe<F> t = MUL::mul(s1, ppp);
+    r.x = fe_sub(fe_sub(fe_sub(MUL::mul(R, R), ppp), Q), Q);
+    r.y = fe_sub(MUL::mul(R, fe_sub(Q, r.x)), t);
     return r;
 }
 
@@ -916,7 +935,7 @@ __device__ __forceinline__ Fq fq_r3() { return fe_rcube<FqP>(); }
 
 // Canonical affine form; identity -> (0, 0).  Latency-optimised (binary
 // inversion): used once per MSM result.
-template <class F>
+template <class F, class MUL = MulInline>
 __device__ __forceinline__ AffineT<F> xyzz_to_affine_fast(const XyzzT<F> &p) {
     AffineT<F> r;
     if (xyzz_is_identity(p)) {
@@ -925,9 +944,10 @@ __device__ __forceinline__ AffineT<F> xyzz_to_affine_fast(const XyzzT<F> &p) {
         return r;
     }
     Fe<F> a = fe_inv_binary<F>(p.zzz, fe_rcube<F>());
-    Fe<F> b = fe_sqr(fe_mul(p.zz, a));
-    r.x = fe_canon(fe_mul(p.x, b));
-    r.y = fe_canon(fe_mul(p.y, a));
+    Fe<F> zza = MUL::mul(p.zz, a);
+    Fe<F> b = MUL::mul(zza, zza);
+    r.x = fe_canon(MUL::mul(p.x, b));
+    r.y = fe_canon(MUL::mul(p.y, a));
     return r;
 }
 

@@ -166,32 +166,15 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     p.ntiles = p.nb_pad / SCAN_TILE;
     p.max_entries = entries;
 
-    // reduce: chunk length per thread, partial-sum slots per window.  The
-    // tail is a chain of dependent point additions: about 2L + log2 L per
-    // reduce lane, and 3 per warp partial in each k_window_sum thread's group
-    // (ceil(buckets / (32 L * 256)) partials).  Pick the L that minimises that
-    // depth for the largest window, with at most sms * 256 reduce lanes:
-    // beyond that the lanes compete for issue slots and the chain length no
-    // longer sets the time (measured on B200: 2^19 buckets reduce in 0.42 ms
-    // with L = 16 and 0.66 ms with L = 8).
-    const u64 target = (u64)sms * 256;
-    u64 wmax_buckets = 1;
-    for (const WinDesc &w : wins) wmax_buckets = std::max<u64>(wmax_buckets, w.nbuckets);
+    // reduce: chunk length L per lane, partial-sum slots per window.  Each
+    // lane runs a chain of about 2L + log2 L dependent point additions, the
+    // reduction tree after it about 15 per level; L is the smallest power of
+    // two that keeps the lanes at most REDUCE_LANES_PER_SM per SM: beyond
+    // that the lanes compete for issue slots and the chain length no longer
+    // sets the time.
+    const u64 target = (u64)sms * REDUCE_LANES_PER_SM;
     u32 L = 1;
     while (nb / L > target && L < (1u << 30)) L <<= 1;
-    {
-        u32 best = L;
-        double best_cost = 1e300;
-        for (u32 l = L; l <= (1u << 20) && l <= wmax_buckets; l <<= 1) {
-            const double groups = std::ceil((double)wmax_buckets / (32.0 * l * WSUM_BLOCK));
-            const double cost = 2.0 * l + std::log2((double)l) + 3.0 * groups;
-            if (cost < best_cost) {
-                best_cost = cost;
-                best = l;
-            }
-        }
-        L = best;
-    }
     std::vector<uint2> rblocks;
     u32 nparts = 0;
     for (u32 wi = 0; wi < wins.size(); wi++) {

@@ -664,13 +664,17 @@ __global__ void __launch_bounds__(AccumShape<C>::threads, AccumShape<C>::per_sm)
     for (u32 pos = start; pos < end; pos++) {
         AffineT<FQ> q = nxt;
         if (pos + 1 < end) nxt = load_entry_point<C>(a.points, a.entries[pos + 1]);
+        // One mixed-addition code path for every entry: a bucket start only
+        // picks the value the addition starts from (lanes of a warp start
+        // buckets at different entries, and a second inlined addition on
+        // that branch would run divergently, doubling the loop's time).
         if (fresh) {
-            acc = (a.carry_in && bbeg >= start) ? xyzz_add_affine(xyzz_load<FQ>(a.buckets + (size_t)b * C::XW), q)
-                                                : xyzz_from_affine(q);
+            acc = (a.carry_in && bbeg >= start) ? xyzz_load<FQ>(a.buckets + (size_t)b * C::XW) : xyzz_identity<FQ>();
             fresh = false;
-        } else {
-            acc = xyzz_add_affine(acc, q);
         }
+        acc = xyzz_add_affine(acc, q);
+        if (a.carry_in && pos + 2 == seg_end && seg_end == bend && b + 1 < a.nb)
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(a.buckets + (size_t)(b + 1) * C::XW));
         if (pos + 1 == seg_end) {
             if (bbeg >= start && bend <= end) {
                 xyzz_store(a.buckets + (size_t)b * C::XW, acc);
@@ -771,7 +775,24 @@ struct ReduceArgs {
     u32 dense;            // 1: every bucket holds a point (identity when empty); ignore offsets
 };
 
+// Products of the tail kernels that run only a few warps (tree levels,
+// final): one out-of-line copy (MulCall); k_reduce runs a few warps per SM.
+#ifndef TAIL_MUL_POLICY
+#define TAIL_MUL_POLICY MulCall
+#endif
+#ifndef REDUCE_MUL_POLICY
+#define REDUCE_MUL_POLICY MulInline
+#endif
+using TailMul = TAIL_MUL_POLICY;
+using ReduceMul = REDUCE_MUL_POLICY;
+
 static constexpr u32 REDUCE_BLOCK = 128;
+#ifndef REDUCE_BLOCKS_PER_SM
+#define REDUCE_BLOCKS_PER_SM 3
+#endif
+#ifndef REDUCE_LANES_PER_SM
+#define REDUCE_LANES_PER_SM 256
+#endif
 static constexpr u32 REDUCE_WARPS = REDUCE_BLOCK / 32;
 
 __device__ __forceinline__ u32 ilog2(u32 x) { return 31 - __clz(x); }
@@ -780,7 +801,7 @@ __device__ __forceinline__ u32 ilog2(u32 x) { return 31 - __clz(x); }
 // values fit in registers (254 instead of 168: spills 2 KB -> 80 B, 4 %
 // faster).
 template <class C>
-__global__ void __launch_bounds__(REDUCE_BLOCK, C::XW == 32 ? 3 : 2) k_reduce(ReduceArgs r) {
+__global__ void __launch_bounds__(REDUCE_BLOCK, C::XW == 32 ? REDUCE_BLOCKS_PER_SM : 2) k_reduce(ReduceArgs r) {
     using FQ = typename C::Fq;
     using Xz = XyzzT<FQ>;
     const uint2 blk = r.blocks[blockIdx.x];
@@ -794,8 +815,8 @@ __global__ void __launch_bounds__(REDUCE_BLOCK, C::XW == 32 ? 3 : 2) k_reduce(Re
         for (u32 k = hi; k > lo; k--) {
             const u32 g = wd.bucket_base + k - 1;
             if (r.dense || r.offsets[g + 1] != r.offsets[g])
-                sum = xyzz_add(sum, xyzz_load<FQ>(r.buckets + (size_t)g * C::XW));
-            sos = xyzz_add(sos, sum);
+                sum = xyzz_add<FQ, ReduceMul>(sum, xyzz_load<FQ>(r.buckets + (size_t)g * C::XW));
+            sos = xyzz_add<FQ, ReduceMul>(sos, sum);
         }
     }
     // inclusive suffix of `sum` inside the warp
@@ -803,14 +824,14 @@ __global__ void __launch_bounds__(REDUCE_BLOCK, C::XW == 32 ? 3 : 2) k_reduce(Re
 #pragma unroll 1
     for (u32 o = 1; o < 32; o <<= 1) {
         Xz y = xyzz_shfl_down(x, o);
-        if (lane + o < 32) x = xyzz_add(x, y);
+        if (lane + o < 32) x = xyzz_add<FQ, ReduceMul>(x, y);
     }
     Xz ex = xyzz_shfl_down(x, 1);
     if (lane == 31) ex = xyzz_identity<FQ>();
-    for (u32 k = 0, lg = ilog2(wd.chunk); k < lg; k++) ex = xyzz_dbl(ex);
-    Xz v = xyzz_add(sos, ex);
+    for (u32 k = 0, lg = ilog2(wd.chunk); k < lg; k++) ex = xyzz_dbl<FQ, ReduceMul>(ex);
+    Xz v = xyzz_add<FQ, ReduceMul>(sos, ex);
 #pragma unroll 1
-    for (u32 o = 16; o; o >>= 1) v = xyzz_add(v, xyzz_shfl_down(v, o));
+    for (u32 o = 16; o; o >>= 1) v = xyzz_add<FQ, ReduceMul>(v, xyzz_shfl_down(v, o));
     if (lane == 0) {
         const size_t slot = (size_t)(wd.part_base + blk.y * REDUCE_WARPS + wid) * C::XW;
         xyzz_store(r.parts_v + slot, v);
@@ -851,16 +872,16 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
     Xz vsum = xyzz_identity<FQ>(), ssum = xyzz_identity<FQ>(), sos = xyzz_identity<FQ>();
     for (u32 b = top; b > b0; b--) {
         const size_t slot = (size_t)(wd.part_base + b - 1) * C::XW;
-        if (b < top) sos = xyzz_add(sos, ssum);
-        vsum = xyzz_add(vsum, xyzz_load<FQ>(a.parts_v + slot));
-        ssum = xyzz_add(ssum, xyzz_load<FQ>(a.parts_s + slot));
+        if (b < top) sos = xyzz_add<FQ, ReduceMul>(sos, ssum);
+        vsum = xyzz_add<FQ, ReduceMul>(vsum, xyzz_load<FQ>(a.parts_v + slot));
+        ssum = xyzz_add<FQ, ReduceMul>(ssum, xyzz_load<FQ>(a.parts_s + slot));
     }
     // block-wide inclusive suffix of ssum: warp scan, then a scan of the warp totals
     Xz x = ssum;
 #pragma unroll 1
     for (u32 o = 1; o < 32; o <<= 1) {
         Xz y = xyzz_shfl_down(x, o);
-        if (lane + o < 32) x = xyzz_add(x, y);
+        if (lane + o < 32) x = xyzz_add<FQ, ReduceMul>(x, y);
     }
     if (lane == 0) xyzz_store(&sm_a[wid][0], x);
     __syncthreads();
@@ -869,7 +890,7 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
 #pragma unroll 1
         for (u32 o = 1; o < WSUM_WARPS; o <<= 1) {
             Xz y = xyzz_shfl_down(t, o);
-            if (lane + o < WSUM_WARPS) t = xyzz_add(t, y);
+            if (lane + o < WSUM_WARPS) t = xyzz_add<FQ, ReduceMul>(t, y);
         }
         if (lane < WSUM_WARPS) xyzz_store(&sm_b[lane][0], t);  // suffix over warps >= lane
     }
@@ -877,13 +898,13 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
     Xz later = wid + 1 < WSUM_WARPS ? xyzz_load<FQ>(&sm_b[wid + 1][0]) : xyzz_identity<FQ>();
     Xz ex = xyzz_shfl_down(x, 1);
     if (lane == 31) ex = xyzz_identity<FQ>();
-    ex = xyzz_add(ex, later);
-    for (u32 k = 0, lg = ilog2(g); k < lg; k++) ex = xyzz_dbl(ex);
-    Xz rs = xyzz_add(sos, ex);  // this group's share of sum_w w * S_w
+    ex = xyzz_add<FQ, ReduceMul>(ex, later);
+    for (u32 k = 0, lg = ilog2(g); k < lg; k++) ex = xyzz_dbl<FQ, ReduceMul>(ex);
+    Xz rs = xyzz_add<FQ, ReduceMul>(sos, ex);  // this group's share of sum_w w * S_w
 #pragma unroll 1
     for (u32 o = 16; o; o >>= 1) {
-        rs = xyzz_add(rs, xyzz_shfl_down(rs, o));
-        vsum = xyzz_add(vsum, xyzz_shfl_down(vsum, o));
+        rs = xyzz_add<FQ, ReduceMul>(rs, xyzz_shfl_down(rs, o));
+        vsum = xyzz_add<FQ, ReduceMul>(vsum, xyzz_shfl_down(vsum, o));
     }
     __syncthreads();
     if (lane == 0) {
@@ -896,13 +917,13 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
         Xz v2 = lane < WSUM_WARPS ? xyzz_load<FQ>(&sm_b[lane][0]) : xyzz_identity<FQ>();
 #pragma unroll 1
         for (u32 o = WSUM_WARPS / 2; o; o >>= 1) {
-            r2 = xyzz_add(r2, xyzz_shfl_down(r2, o));
-            v2 = xyzz_add(v2, xyzz_shfl_down(v2, o));
+            r2 = xyzz_add<FQ, ReduceMul>(r2, xyzz_shfl_down(r2, o));
+            v2 = xyzz_add<FQ, ReduceMul>(v2, xyzz_shfl_down(v2, o));
         }
         if (lane == 0) {
             const u32 shift = ilog2(wd.chunk) + 5;  // 32 lanes per warp partial
-            for (u32 k = 0; k < shift; k++) r2 = xyzz_dbl(r2);
-            xyzz_store(a.wres + (size_t)win * C::XW, xyzz_add(v2, r2));
+            for (u32 k = 0; k < shift; k++) r2 = xyzz_dbl<FQ, ReduceMul>(r2);
+            xyzz_store(a.wres + (size_t)win * C::XW, xyzz_add<FQ, ReduceMul>(v2, r2));
         }
     }
 }
@@ -954,17 +975,17 @@ __global__ void __launch_bounds__(TREE_BLOCK, C::XW == 32 ? 2 : 1) k_reduce_tree
 #pragma unroll 1
     for (u32 o = 1; o < 32; o <<= 1) {
         Xz y = xyzz_shfl_down(x, o);
-        if (lane + o < 32) x = xyzz_add(x, y);
+        if (lane + o < 32) x = xyzz_add<FQ, TailMul>(x, y);
     }
     Xz w = lane ? x : xyzz_identity<FQ>();
 #pragma unroll 1
     for (u32 o = 16; o; o >>= 1) {
-        A = xyzz_add(A, xyzz_shfl_down(A, o));
-        w = xyzz_add(w, xyzz_shfl_down(w, o));
+        A = xyzz_add<FQ, TailMul>(A, xyzz_shfl_down(A, o));
+        w = xyzz_add<FQ, TailMul>(w, xyzz_shfl_down(w, o));
     }
     if (lane == 0) {
-        for (u32 k = 0; k < gr.shift; k++) w = xyzz_dbl(w);
-        A = xyzz_add(A, w);
+        for (u32 k = 0; k < gr.shift; k++) w = xyzz_dbl<FQ, TailMul>(w);
+        A = xyzz_add<FQ, TailMul>(A, w);
         if (gr.out & TREE_FINAL) {
             xyzz_store(a.wres + (size_t)(gr.out & ~TREE_FINAL) * C::XW, A);
         } else {
@@ -994,12 +1015,12 @@ __global__ void k_final(FinalArgs f) {
     XyzzT<FQ> acc = xyzz_identity<FQ>();
     for (int w = (int)d.n_windows - 1; w >= 0; w--) {
         if (!xyzz_is_identity(acc))
-            for (u32 k = 0; k < d.c; k++) acc = xyzz_dbl(acc);
-        acc = xyzz_add(acc, xyzz_load<FQ>(f.wres + (size_t)(d.win_base + w) * C::XW));
+            for (u32 k = 0; k < d.c; k++) acc = xyzz_dbl<FQ, TailMul>(acc);
+        acc = xyzz_add<FQ, TailMul>(acc, xyzz_load<FQ>(f.wres + (size_t)(d.win_base + w) * C::XW));
     }
-    if (f.carry) acc = xyzz_add(acc, xyzz_load<FQ>(f.carry + (size_t)m * C::XW));
+    if (f.carry) acc = xyzz_add<FQ, TailMul>(acc, xyzz_load<FQ>(f.carry + (size_t)m * C::XW));
     if (f.emit_affine) {
-        affine_store(f.results + (size_t)m * C::PW, xyzz_to_affine_fast(acc));
+        affine_store(f.results + (size_t)m * C::PW, xyzz_to_affine_fast<FQ, TailMul>(acc));
     } else {
         xyzz_store(f.carry + (size_t)m * C::XW, acc);
     }
@@ -1011,8 +1032,8 @@ __global__ void k_combine(const u32 *xyzz, u32 k, u32 *out) {
     using FQ = typename C::Fq;
     if (blockIdx.x || threadIdx.x) return;
     XyzzT<FQ> acc = xyzz_identity<FQ>();
-    for (u32 i = 0; i < k; i++) acc = xyzz_add(acc, xyzz_load<FQ>(xyzz + (size_t)i * C::XW));
-    affine_store(out, xyzz_to_affine_fast(acc));
+    for (u32 i = 0; i < k; i++) acc = xyzz_add<FQ, TailMul>(acc, xyzz_load<FQ>(xyzz + (size_t)i * C::XW));
+    affine_store(out, xyzz_to_affine_fast<FQ, TailMul>(acc));
 }
 
 }  // namespace impeller
