@@ -70,31 +70,51 @@ struct WinDesc {
 // a digit >= 2^(c-1) becomes digit - 2^c and carries into the next window.
 // The top window is never recoded: for every 3 <= c <= 31, r < 2^254 keeps
 // the top digit plus an incoming carry at most 2^(c-1), a valid bucket.
-// Windows are taken in order, w = 0, 1, ...: the scalar is shifted right by
-// c after each window, so the next digit is always the low c bits of limb 0.
-template <class FR>
-struct DigitIter {
-    Fe<FR> v;
-    u32 c, carry;
-    __device__ __forceinline__ void next(u32 w, u32 n_logical, u32 &mag, u32 &sign) {
-        const u32 raw = v.l[0] & ((1u << c) - 1u);
-#pragma unroll
-        for (int k = 0; k < 7; k++) v.l[k] = __funnelshift_r(v.l[k], v.l[k + 1], c);
-        v.l[7] >>= c;
-        u32 d = raw + carry;
-        u32 half = 1u << (c - 1);
-        if (d >= half && w + 1 < n_logical) {
-            // d >= 2^(c-1) on a non-top window: negative digit d - 2^c
-            mag = (1u << c) - d;
-            sign = 1;
+//
+// for_each_digit calls emit(pw, table, mag, sign) for each of the n_logical
+// digit windows w of a canonical scalar, lowest first (mag == 0 for a zero
+// digit), with pw = w mod n_windows (the bucket set) and table = w /
+// n_windows (the window table).  The scalar's limbs feed a 64-bit bit buffer
+// one at a time -- the limb index is a constant in every unrolled step -- so
+// a digit costs one 64-bit shift, and the window and table indices advance
+// by counting instead of dividing.  Every lane runs the same windows (the
+// count depends only on c and n_logical).
+template <class FR, class Emit>
+__device__ __forceinline__ void for_each_digit(const Fe<FR> &v, u32 c, u32 n_logical, u32 n_windows, Emit &&emit) {
+    const u32 mask = (1u << c) - 1u, half = 1u << (c - 1);
+    u64 buf = 0;
+    u32 nbits = 0, carry = 0, w = 0, pw = 0, table = 0;
+    auto step = [&](u32 raw, bool top) {
+        const u32 d = raw + carry;
+        if (d >= half && !top) {
+            emit(pw, table, (1u << c) - d, 1u);
             carry = 1;
         } else {
-            mag = d;
-            sign = 0;
+            emit(pw, table, d, 0u);
             carry = 0;
         }
+        w++;
+        if (++pw == n_windows) {
+            pw = 0;
+            table++;
+        }
+    };
+#pragma unroll
+    for (int k = 0; k < FR::N; k++) {
+        buf |= (u64)v.l[k] << nbits;
+        nbits += 32;
+        while (nbits >= c && w + 1 < n_logical) {
+            step((u32)buf & mask, false);
+            buf >>= c;
+            nbits -= c;
+        }
     }
-};
+    while (w + 1 < n_logical) {
+        step((u32)buf & mask, false);
+        buf >>= c;
+    }
+    step((u32)buf & mask, true);
+}
 
 // Lanes of a warp whose digits hit the same bucket share one atomic: heavy
 // buckets (the top window in a shared bucket set, the 0 / 1 / small scalars of
@@ -110,18 +130,13 @@ __global__ void k_histogram(const MsmDesc *__restrict__ descs, u32 *__restrict__
     for (u32 base = blockIdx.x * blockDim.x; base < d.n; base += stride) {
         const u32 i = base + threadIdx.x;
         const bool live = i < d.n;
-        DigitIter<typename C::Fr> it;
-        it.v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
-                    : fe_zero<typename C::Fr>();
-        it.c = d.c;
-        it.carry = 0;
-        for (u32 w = 0; w < d.n_logical; w++) {
-            u32 mag, sign;
-            it.next(w, d.n_logical, mag, sign);
-            const u32 key = mag ? d.bucket_base + (w % d.n_windows) * B + mag - 1 : NONE;
+        const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
+                                          : fe_zero<typename C::Fr>();
+        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
+            const u32 key = mag ? d.bucket_base + pw * B + mag - 1 : NONE;
             const u32 peers = __match_any_sync(0xffffffffu, key);
             if (key != NONE && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (u32)__popc(peers));
-        }
+        });
     }
 }
 
@@ -134,15 +149,10 @@ __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ c
     for (u32 base = blockIdx.x * blockDim.x; base < d.n; base += stride) {
         const u32 i = base + threadIdx.x;
         const bool live = i < d.n;
-        DigitIter<typename C::Fr> it;
-        it.v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
-                    : fe_zero<typename C::Fr>();
-        it.c = d.c;
-        it.carry = 0;
-        for (u32 w = 0; w < d.n_logical; w++) {
-            u32 mag, sign;
-            it.next(w, d.n_logical, mag, sign);
-            const u32 key = mag ? d.bucket_base + (w % d.n_windows) * B + mag - 1 : NONE;
+        const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
+                                          : fe_zero<typename C::Fr>();
+        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
+            const u32 key = mag ? d.bucket_base + pw * B + mag - 1 : NONE;
             const u32 peers = __match_any_sync(0xffffffffu, key);
             const u32 leader = __ffs(peers) - 1;
             u32 pos = 0;
@@ -150,10 +160,9 @@ __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ c
             pos = __shfl_sync(0xffffffffu, pos, leader);
             if (key != NONE) {
                 const u32 rank = __popc(peers & ((1u << lane) - 1u));
-                const u32 table = w / d.n_windows;
                 entries[pos + rank] = ((d.table_base + table * d.table_stride + i) << 1) | sign;
             }
-        }
+        });
     }
 }
 
@@ -261,16 +270,11 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
     for (u32 base = start; base < end; base += blockDim.x) {
         const u32 i = base + threadIdx.x;
         const bool live = i < end;
-        DigitIter<typename C::Fr> it;
-        it.v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
-                    : fe_zero<typename C::Fr>();
-        it.c = d.c;
-        it.carry = 0;
-        for (u32 w = 0; w < d.n_logical; w++) {
-            u32 mag, sign;
-            it.next(w, d.n_logical, mag, sign);
-            if (mag) atomicAdd(&hist[(d.bucket_base + (w % d.n_windows) * B + mag - 1) >> FINE_BITS], 1u);
-        }
+        const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
+                                          : fe_zero<typename C::Fr>();
+        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
+            if (mag) atomicAdd(&hist[(d.bucket_base + pw * B + mag - 1) >> FINE_BITS], 1u);
+        });
     }
     __syncthreads();
     for (u32 b = threadIdx.x; b < a.nbins; b += blockDim.x) a.cnt[(size_t)b * a.ntiles + blockIdx.x] = hist[b];
@@ -316,22 +320,16 @@ __global__ void __launch_bounds__(SORT_BLOCK, 2) k_coarse_scatter(SortArgs a) {
     for (u32 base = start; base < end; base += blockDim.x) {
         const u32 i = base + threadIdx.x;
         const bool live = i < end;
-        DigitIter<typename C::Fr> it;
-        it.v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
-                    : fe_zero<typename C::Fr>();
-        it.c = d.c;
-        it.carry = 0;
-        for (u32 w = 0; w < d.n_logical; w++) {
-            u32 mag, sign;
-            it.next(w, d.n_logical, mag, sign);
+        const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
+                                          : fe_zero<typename C::Fr>();
+        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
             if (mag) {
-                const u32 key = d.bucket_base + (w % d.n_windows) * B + mag - 1;
+                const u32 key = d.bucket_base + pw * B + mag - 1;
                 const u32 slot = atomicAdd(&cur[key >> FINE_BITS], 1u);
-                const u32 table = w / d.n_windows;
                 stage_e[slot] = ((d.table_base + table * d.table_stride + i) << 1) | sign;
                 stage_f[slot] = (unsigned short)(key & (FINE - 1u));
             }
-        }
+        });
     }
     __syncthreads();
     // one warp per bin writes the bin's run of this tile: one coalesced run
@@ -775,20 +773,31 @@ struct ReduceArgs {
     u32 dense;            // 1: every bucket holds a point (identity when empty); ignore offsets
 };
 
-// Products of the tail kernels that run only a few warps (tree levels,
-// final): one out-of-line copy (MulCall); k_reduce runs a few warps per SM.
+// Products of the reduction-tree levels, which run one to a few dozen
+// warps of straight-line point additions: one out-of-line copy (MulCall),
+// 11 % faster than inlined at 2^19 buckets on B200.  k_final's Horner loop
+// repeats one doubling, whose inlined code stays in the instruction cache:
+// inlined there (8 % faster than out-of-line at window 17).  k_reduce runs
+// a few warps per SM: inlined (out-of-line measured 10-19 % slower).
 #ifndef TAIL_MUL_POLICY
 #define TAIL_MUL_POLICY MulCall
+#endif
+#ifndef FINAL_MUL_POLICY
+#define FINAL_MUL_POLICY MulInline
 #endif
 #ifndef REDUCE_MUL_POLICY
 #define REDUCE_MUL_POLICY MulInline
 #endif
 using TailMul = TAIL_MUL_POLICY;
+using FinalMul = FINAL_MUL_POLICY;
 using ReduceMul = REDUCE_MUL_POLICY;
 
 static constexpr u32 REDUCE_BLOCK = 128;
+// Two 128-thread CTAs per SM (190 registers, no spills): the reduce grid
+// fills fewer than two per SM at 2^19 buckets anyway; three (168 registers,
+// 356 bytes of spills) measured 1-2 % slower.
 #ifndef REDUCE_BLOCKS_PER_SM
-#define REDUCE_BLOCKS_PER_SM 3
+#define REDUCE_BLOCKS_PER_SM 2
 #endif
 #ifndef REDUCE_LANES_PER_SM
 #define REDUCE_LANES_PER_SM 256
@@ -797,9 +806,8 @@ static constexpr u32 REDUCE_WARPS = REDUCE_BLOCK / 32;
 
 __device__ __forceinline__ u32 ilog2(u32 x) { return 31 - __clz(x); }
 
-// Three CTAs per SM on BN254; on BLS12-381 two, so that the 48-word XYZZ
-// values fit in registers (254 instead of 168: spills 2 KB -> 80 B, 4 %
-// faster).
+// On BLS12-381 two CTAs per SM, so that the 48-word XYZZ values fit in
+// registers (254 instead of 168: spills 2 KB -> 80 B, 4 % faster).
 template <class C>
 __global__ void __launch_bounds__(REDUCE_BLOCK, C::XW == 32 ? REDUCE_BLOCKS_PER_SM : 2) k_reduce(ReduceArgs r) {
     using FQ = typename C::Fq;
@@ -1015,12 +1023,12 @@ __global__ void k_final(FinalArgs f) {
     XyzzT<FQ> acc = xyzz_identity<FQ>();
     for (int w = (int)d.n_windows - 1; w >= 0; w--) {
         if (!xyzz_is_identity(acc))
-            for (u32 k = 0; k < d.c; k++) acc = xyzz_dbl<FQ, TailMul>(acc);
-        acc = xyzz_add<FQ, TailMul>(acc, xyzz_load<FQ>(f.wres + (size_t)(d.win_base + w) * C::XW));
+            for (u32 k = 0; k < d.c; k++) acc = xyzz_dbl<FQ, FinalMul>(acc);
+        acc = xyzz_add<FQ, FinalMul>(acc, xyzz_load<FQ>(f.wres + (size_t)(d.win_base + w) * C::XW));
     }
-    if (f.carry) acc = xyzz_add<FQ, TailMul>(acc, xyzz_load<FQ>(f.carry + (size_t)m * C::XW));
+    if (f.carry) acc = xyzz_add<FQ, FinalMul>(acc, xyzz_load<FQ>(f.carry + (size_t)m * C::XW));
     if (f.emit_affine) {
-        affine_store(f.results + (size_t)m * C::PW, xyzz_to_affine_fast<FQ, TailMul>(acc));
+        affine_store(f.results + (size_t)m * C::PW, xyzz_to_affine_fast<FQ, FinalMul>(acc));
     } else {
         xyzz_store(f.carry + (size_t)m * C::XW, acc);
     }
@@ -1032,8 +1040,8 @@ __global__ void k_combine(const u32 *xyzz, u32 k, u32 *out) {
     using FQ = typename C::Fq;
     if (blockIdx.x || threadIdx.x) return;
     XyzzT<FQ> acc = xyzz_identity<FQ>();
-    for (u32 i = 0; i < k; i++) acc = xyzz_add<FQ, TailMul>(acc, xyzz_load<FQ>(xyzz + (size_t)i * C::XW));
-    affine_store(out, xyzz_to_affine_fast<FQ, TailMul>(acc));
+    for (u32 i = 0; i < k; i++) acc = xyzz_add<FQ, FinalMul>(acc, xyzz_load<FQ>(xyzz + (size_t)i * C::XW));
+    affine_store(out, xyzz_to_affine_fast<FQ, FinalMul>(acc));
 }
 
 }  // namespace impeller
