@@ -1012,6 +1012,19 @@ __device__ __forceinline__ XyzzT<F> xyzz_shfl_down(const XyzzT<F> &p, u32 delta,
     return r;
 }
 
+template <class F>
+__device__ __forceinline__ XyzzT<F> xyzz_shfl_xor(const XyzzT<F> &p, u32 lane_mask) {
+    XyzzT<F> r;
+#pragma unroll
+    for (int i = 0; i < F::N; i++) {
+        r.x.l[i] = __shfl_xor_sync(0xffffffffu, p.x.l[i], lane_mask);
+        r.y.l[i] = __shfl_xor_sync(0xffffffffu, p.y.l[i], lane_mask);
+        r.zz.l[i] = __shfl_xor_sync(0xffffffffu, p.zz.l[i], lane_mask);
+        r.zzz.l[i] = __shfl_xor_sync(0xffffffffu, p.zzz.l[i], lane_mask);
+    }
+    return r;
+}
+
 // k * p for a small plain scalar k, left-to-right double-and-add.
 template <class F>
 __device__ __forceinline__ XyzzT<F> xyzz_mul_u32(const XyzzT<F> &p, u32 k) {

@@ -986,14 +986,17 @@ __global__ void __launch_bounds__(TREE_BLOCK, C::XW == 32 ? 2 : 1) k_reduce_tree
         if (lane + o < 32) x = xyzz_add<FQ, TailMul>(x, y);
     }
     Xz w = lane ? x : xyzz_identity<FQ>();
+    // The sums of A and of w over the warp: the first step folds lanes l and
+    // l + 16 so that lanes 0-15 carry partial sums of A and lanes 16-31 of w,
+    // then each half reduces on its own -- one addition per step, not two.
+    Xz v = xyzz_add<FQ, TailMul>(lane < 16 ? A : w, xyzz_shfl_xor(lane < 16 ? w : A, 16));
 #pragma unroll 1
-    for (u32 o = 16; o; o >>= 1) {
-        A = xyzz_add<FQ, TailMul>(A, xyzz_shfl_down(A, o));
-        w = xyzz_add<FQ, TailMul>(w, xyzz_shfl_down(w, o));
-    }
+    for (u32 o = 8; o; o >>= 1) v = xyzz_add<FQ, TailMul>(v, xyzz_shfl_xor(v, o));
+    if (lane == 16)
+        for (u32 k = 0; k < gr.shift; k++) v = xyzz_dbl<FQ, TailMul>(v);
+    w = xyzz_shfl_down(v, 16);
     if (lane == 0) {
-        for (u32 k = 0; k < gr.shift; k++) w = xyzz_dbl<FQ, TailMul>(w);
-        A = xyzz_add<FQ, TailMul>(A, w);
+        A = xyzz_add<FQ, TailMul>(v, w);
         if (gr.out & TREE_FINAL) {
             xyzz_store(a.wres + (size_t)(gr.out & ~TREE_FINAL) * C::XW, A);
         } else {
