@@ -359,6 +359,185 @@ __device__ __forceinline__ void bn_row_reduce(u32 (&x)[8], u32 (&y)[8]) {
           "n"(F::INV));
 }
 
+// Square of an 8-word value, all 16 words: the 28 cross products a_i a_j
+// (i < j) go into two accumulators of register pairs -- E on even-aligned
+// pairs, O on odd-aligned ones -- so that every lo/hi multiply-add lands on
+// an aligned pair; each row's chain ends on a word no earlier row wrote, or
+// hands its carry to the next such word.  Then t = 2 (E + O) + sum a_i^2
+// 2^(64 i).  36 products where a general product of two values takes 64.
+__device__ __forceinline__ void bn_sqr_wide(u32 (&t)[16], const u32 (&a)[8]) {
+    asm(
+        "{\n\t.reg .u32 E2, E3, E4, E5, E6, E7, E8, E9, E10, E11, E12, E13, O1, O2, O3, O4, O5, O6, O7, O8, O9, O10, O11, O12, O13, O14;\n\t"
+        "mul.lo.u32 O1, %16, %17;\n\t"
+        "mul.hi.u32 O2, %16, %17;\n\t"
+        "mul.lo.u32 O3, %16, %19;\n\t"
+        "mul.hi.u32 O4, %16, %19;\n\t"
+        "mul.lo.u32 O5, %16, %21;\n\t"
+        "mul.hi.u32 O6, %16, %21;\n\t"
+        "mul.lo.u32 O7, %16, %23;\n\t"
+        "mul.hi.u32 O8, %16, %23;\n\t"
+        "mul.lo.u32 E2, %16, %18;\n\t"
+        "mul.hi.u32 E3, %16, %18;\n\t"
+        "mul.lo.u32 E4, %16, %20;\n\t"
+        "mul.hi.u32 E5, %16, %20;\n\t"
+        "mul.lo.u32 E6, %16, %22;\n\t"
+        "mul.hi.u32 E7, %16, %22;\n\t"
+        "mad.lo.cc.u32 O3, %17, %18, O3;\n\t"
+        "madc.hi.cc.u32 O4, %17, %18, O4;\n\t"
+        "madc.lo.cc.u32 O5, %17, %20, O5;\n\t"
+        "madc.hi.cc.u32 O6, %17, %20, O6;\n\t"
+        "madc.lo.cc.u32 O7, %17, %22, O7;\n\t"
+        "madc.hi.cc.u32 O8, %17, %22, O8;\n\t"
+        "addc.u32 O9, 0, 0;\n\t"
+        "mad.lo.cc.u32 E4, %17, %19, E4;\n\t"
+        "madc.hi.cc.u32 E5, %17, %19, E5;\n\t"
+        "madc.lo.cc.u32 E6, %17, %21, E6;\n\t"
+        "madc.hi.cc.u32 E7, %17, %21, E7;\n\t"
+        "madc.lo.cc.u32 E8, %17, %23, 0;\n\t"
+        "madc.hi.u32 E9, %17, %23, 0;\n\t"
+        "mad.lo.cc.u32 O5, %18, %19, O5;\n\t"
+        "madc.hi.cc.u32 O6, %18, %19, O6;\n\t"
+        "madc.lo.cc.u32 O7, %18, %21, O7;\n\t"
+        "madc.hi.cc.u32 O8, %18, %21, O8;\n\t"
+        "madc.lo.cc.u32 O9, %18, %23, O9;\n\t"
+        "madc.hi.u32 O10, %18, %23, 0;\n\t"
+        "mad.lo.cc.u32 E6, %18, %20, E6;\n\t"
+        "madc.hi.cc.u32 E7, %18, %20, E7;\n\t"
+        "madc.lo.cc.u32 E8, %18, %22, E8;\n\t"
+        "madc.hi.cc.u32 E9, %18, %22, E9;\n\t"
+        "addc.u32 E10, 0, 0;\n\t"
+        "mad.lo.cc.u32 O7, %19, %20, O7;\n\t"
+        "madc.hi.cc.u32 O8, %19, %20, O8;\n\t"
+        "madc.lo.cc.u32 O9, %19, %22, O9;\n\t"
+        "madc.hi.cc.u32 O10, %19, %22, O10;\n\t"
+        "addc.u32 O11, 0, 0;\n\t"
+        "mad.lo.cc.u32 E8, %19, %21, E8;\n\t"
+        "madc.hi.cc.u32 E9, %19, %21, E9;\n\t"
+        "madc.lo.cc.u32 E10, %19, %23, E10;\n\t"
+        "madc.hi.u32 E11, %19, %23, 0;\n\t"
+        "mad.lo.cc.u32 O9, %20, %21, O9;\n\t"
+        "madc.hi.cc.u32 O10, %20, %21, O10;\n\t"
+        "madc.lo.cc.u32 O11, %20, %23, O11;\n\t"
+        "madc.hi.u32 O12, %20, %23, 0;\n\t"
+        "mad.lo.cc.u32 E10, %20, %22, E10;\n\t"
+        "madc.hi.cc.u32 E11, %20, %22, E11;\n\t"
+        "addc.u32 E12, 0, 0;\n\t"
+        "mad.lo.cc.u32 O11, %21, %22, O11;\n\t"
+        "madc.hi.cc.u32 O12, %21, %22, O12;\n\t"
+        "addc.u32 O13, 0, 0;\n\t"
+        "mad.lo.cc.u32 E12, %21, %23, E12;\n\t"
+        "madc.hi.u32 E13, %21, %23, 0;\n\t"
+        "mad.lo.cc.u32 O13, %22, %23, O13;\n\t"
+        "madc.hi.u32 O14, %22, %23, 0;\n\t"
+        "add.cc.u32 %1, 0, O1;\n\t"
+        "addc.cc.u32 %2, E2, O2;\n\t"
+        "addc.cc.u32 %3, E3, O3;\n\t"
+        "addc.cc.u32 %4, E4, O4;\n\t"
+        "addc.cc.u32 %5, E5, O5;\n\t"
+        "addc.cc.u32 %6, E6, O6;\n\t"
+        "addc.cc.u32 %7, E7, O7;\n\t"
+        "addc.cc.u32 %8, E8, O8;\n\t"
+        "addc.cc.u32 %9, E9, O9;\n\t"
+        "addc.cc.u32 %10, E10, O10;\n\t"
+        "addc.cc.u32 %11, E11, O11;\n\t"
+        "addc.cc.u32 %12, E12, O12;\n\t"
+        "addc.cc.u32 %13, E13, O13;\n\t"
+        "addc.cc.u32 %14, 0, O14;\n\t"
+        "addc.u32 %15, 0, 0;\n\t"
+        "add.cc.u32 %1, %1, %1;\n\t"
+        "addc.cc.u32 %2, %2, %2;\n\t"
+        "addc.cc.u32 %3, %3, %3;\n\t"
+        "addc.cc.u32 %4, %4, %4;\n\t"
+        "addc.cc.u32 %5, %5, %5;\n\t"
+        "addc.cc.u32 %6, %6, %6;\n\t"
+        "addc.cc.u32 %7, %7, %7;\n\t"
+        "addc.cc.u32 %8, %8, %8;\n\t"
+        "addc.cc.u32 %9, %9, %9;\n\t"
+        "addc.cc.u32 %10, %10, %10;\n\t"
+        "addc.cc.u32 %11, %11, %11;\n\t"
+        "addc.cc.u32 %12, %12, %12;\n\t"
+        "addc.cc.u32 %13, %13, %13;\n\t"
+        "addc.cc.u32 %14, %14, %14;\n\t"
+        "addc.u32 %15, %15, %15;\n\t"
+        "mul.lo.u32 %0, %16, %16;\n\t"
+        "mad.hi.cc.u32 %1, %16, %16, %1;\n\t"
+        "madc.lo.cc.u32 %2, %17, %17, %2;\n\t"
+        "madc.hi.cc.u32 %3, %17, %17, %3;\n\t"
+        "madc.lo.cc.u32 %4, %18, %18, %4;\n\t"
+        "madc.hi.cc.u32 %5, %18, %18, %5;\n\t"
+        "madc.lo.cc.u32 %6, %19, %19, %6;\n\t"
+        "madc.hi.cc.u32 %7, %19, %19, %7;\n\t"
+        "madc.lo.cc.u32 %8, %20, %20, %8;\n\t"
+        "madc.hi.cc.u32 %9, %20, %20, %9;\n\t"
+        "madc.lo.cc.u32 %10, %21, %21, %10;\n\t"
+        "madc.hi.cc.u32 %11, %21, %21, %11;\n\t"
+        "madc.lo.cc.u32 %12, %22, %22, %12;\n\t"
+        "madc.hi.cc.u32 %13, %22, %22, %13;\n\t"
+        "madc.lo.cc.u32 %14, %23, %23, %14;\n\t"
+        "madc.hi.u32 %15, %23, %23, %15;\n\t"
+        "}"
+        : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7]),
+          "=r"(t[8]), "=r"(t[9]), "=r"(t[10]), "=r"(t[11]), "=r"(t[12]), "=r"(t[13]), "=r"(t[14]), "=r"(t[15])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]));
+}
+
+// Squaring's reduction row: the division of the running value by 2^32 (the
+// role swap of bn_row_next: x becomes the old Y array, y the old X array two
+// words down, old X_1 added at weight 0), the square's next word w entering
+// at weight 7 (as y_6, a zero word after the shift), and the reduction row of
+// bn_row_reduce, in one carry chain.
+template <class F>
+__device__ __forceinline__ void bn_row_reduce_word(u32 (&x)[8], u32 (&y)[8], u32 w) {
+    asm("{\n\t.reg .u32 m;\n\t"
+        "add.cc.u32     %0, %0, %9;\n\t"
+        "mul.lo.u32     m, %0, %24;\n\t"
+        "madc.lo.cc.u32 %8, m, %17, %10;\n\tmadc.hi.cc.u32 %9, m, %17, %11;\n\t"
+        "madc.lo.cc.u32 %10, m, %19, %12;\n\tmadc.hi.cc.u32 %11, m, %19, %13;\n\t"
+        "madc.lo.cc.u32 %12, m, %21, %14;\n\tmadc.hi.cc.u32 %13, m, %21, %15;\n\t"
+        "madc.lo.cc.u32 %14, m, %23, %25;\n\tmadc.hi.u32    %15, m, %23, 0;\n\t"
+        "mad.lo.cc.u32  %0, m, %16, %0;\n\tmadc.hi.cc.u32 %1, m, %16, %1;\n\t"
+        "madc.lo.cc.u32 %2, m, %18, %2;\n\tmadc.hi.cc.u32 %3, m, %18, %3;\n\t"
+        "madc.lo.cc.u32 %4, m, %20, %4;\n\tmadc.hi.cc.u32 %5, m, %20, %5;\n\t"
+        "madc.lo.cc.u32 %6, m, %22, %6;\n\tmadc.hi.cc.u32 %7, m, %22, %7;\n\t"
+        "addc.u32       %15, %15, 0;\n\t}"
+        : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]), "+r"(x[7]),
+          "+r"(y[0]), "+r"(y[1]), "+r"(y[2]), "+r"(y[3]), "+r"(y[4]), "+r"(y[5]), "+r"(y[6]), "+r"(y[7])
+        : "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5), "n"(F::M6), "n"(F::M7),
+          "n"(F::INV), "r"(w));
+}
+
+// Montgomery square a*a*R^{-1} in [0, 2N) for 8-word fields: the full square
+// (bn_sqr_wide), then eight reduction rows over it, its upper words entering
+// one per row.  The same value (a^2 + m N) / R as fe_mul(a, a): m is fixed by
+// a^2 mod R.  259 instructions and 36 + 64 products against 280 and 64 + 64.
+template <class F>
+__device__ __forceinline__ Fe<F> fe_sqr_inline(const Fe<F> &a) {
+    u32 t[16];
+    bn_sqr_wide(t, a.l);
+    u32 u[8] = {t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7]}, v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bn_row_reduce<F>(u, v);
+    bn_row_reduce_word<F>(v, u, t[8]);
+    bn_row_reduce_word<F>(u, v, t[9]);
+    bn_row_reduce_word<F>(v, u, t[10]);
+    bn_row_reduce_word<F>(u, v, t[11]);
+    bn_row_reduce_word<F>(v, u, t[12]);
+    bn_row_reduce_word<F>(u, v, t[13]);
+    bn_row_reduce_word<F>(v, u, t[14]);
+    Fe<F> r;
+    asm("add.cc.u32  %0, %8, %16;\n\taddc.cc.u32 %1, %9, %17;\n\taddc.cc.u32 %2, %10, %18;\n\t"
+        "addc.cc.u32 %3, %11, %19;\n\taddc.cc.u32 %4, %12, %20;\n\taddc.cc.u32 %5, %13, %21;\n\t"
+        "addc.cc.u32 %6, %14, %22;\n\taddc.u32    %7, %15, %23;"
+        : "=r"(r.l[0]), "=r"(r.l[1]), "=r"(r.l[2]), "=r"(r.l[3]), "=r"(r.l[4]), "=r"(r.l[5]), "=r"(r.l[6]),
+          "=r"(r.l[7])
+        : "r"(u[0]), "r"(u[1]), "r"(u[2]), "r"(u[3]), "r"(u[4]), "r"(u[5]), "r"(u[6]), "r"(u[7]), "r"(v[1]),
+          "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(t[15]));
+    if constexpr (!F::LAZY) {
+        const Fe<F> q = r;
+        fe_reduce_once<F>(r, q.l);
+    }
+    return r;
+}
+
 // Montgomery product a*b*R^{-1} mod N in [0, 2N) for inputs in [0, 2N).
 // Eight rows with the accumulators alternating; after the last (odd) row the
 // value is u_0..7 + v_1..7 (v_0 is zero).  No final subtraction (lazy
@@ -426,9 +605,15 @@ __device__ __forceinline__ Fe<F> fe_mul(Fe<F> a, Fe<F> b) {
     return fe_mul_inline<F>(a, b);
 }
 
+// Squares of 8-word values take the dedicated square (IMPELLER_SQR_AS_MUL
+// selects the general product instead, for comparison builds).
 template <class F>
 __device__ __forceinline__ Fe<F> fe_sqr(const Fe<F> &a) {
-    return fe_mul<F>(a, a);
+#ifndef IMPELLER_SQR_AS_MUL
+    if constexpr (F::N == 8) return fe_sqr_inline<F>(a);
+    else
+#endif
+        return fe_mul<F>(a, a);
 }
 
 // One out-of-line copy of the product, for kernels that run only a few warps
