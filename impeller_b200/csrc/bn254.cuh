@@ -626,13 +626,22 @@ __device__ __noinline__ Fe<F> fe_mul_call(Fe<F> a, Fe<F> b) {
     return fe_mul_inline<F>(a, b);
 }
 
+template <class F>
+__device__ __noinline__ Fe<F> fe_sqr_call(Fe<F> a) {
+    return fe_sqr<F>(a);
+}
+
 struct MulInline {
     template <class F>
     __device__ __forceinline__ static Fe<F> mul(const Fe<F> &a, const Fe<F> &b) { return fe_mul<F>(a, b); }
+    template <class F>
+    __device__ __forceinline__ static Fe<F> sqr(const Fe<F> &a) { return fe_sqr<F>(a); }
 };
 struct MulCall {
     template <class F>
     __device__ __forceinline__ static Fe<F> mul(const Fe<F> &a, const Fe<F> &b) { return fe_mul_call<F>(a, b); }
+    template <class F>
+    __device__ __forceinline__ static Fe<F> sqr(const Fe<F> &a) { return fe_sqr_call<F>(a); }
 };
 
 // Leave Montgomery form: a * R^{-1} mod N, canonical, for a in [0, 2N)
@@ -871,37 +880,56 @@ __device__ __forceinline__ void un_sub(u32 *a, const u32 *b) {
 }
 
 // x = x / 2 mod N for x < 2N (N odd): if x is odd, (x + N) / 2 < 3N / 2.
+// x * 2^-k mod N for 1 <= k <= 32 (x in [0, 2N), or [0, N) on fields
+// without lazy reduction, and the result in the same range): q = -x N^-1
+// mod 2^k makes x + q N divisible by 2^k.
 template <class F>
-__device__ __forceinline__ void fe_half(u32 *x) {
-    if constexpr (F::N == 12) {
-        if (x[0] & 1u) {
-            constexpr Words<12> m = words(F::M);
-            u32 t[12];
-            add12(t, x, m.v);  // x + N < 3N < 2^384
+__device__ __forceinline__ void fe_div2k(u32 *x, u32 k) {
+    constexpr int N = F::N;
+    constexpr Words<N> m = words(F::M);
+    const u32 q = (x[0] * F::INV) & (k == 32 ? 0xffffffffu : ((1u << k) - 1u));
+    u32 t[N + 1];
+    u64 c = 0;
 #pragma unroll
-            for (int i = 0; i < 12; i++) x[i] = t[i];
-        }
-        un_shr1<12>(x, 0);
-    } else if (x[0] & 1u) {
-        u32 c;
-        asm("add.cc.u32  %0, %0, %9;\n\t"
-            "addc.cc.u32 %1, %1, %10;\n\t"
-            "addc.cc.u32 %2, %2, %11;\n\t"
-            "addc.cc.u32 %3, %3, %12;\n\t"
-            "addc.cc.u32 %4, %4, %13;\n\t"
-            "addc.cc.u32 %5, %5, %14;\n\t"
-            "addc.cc.u32 %6, %6, %15;\n\t"
-            "addc.cc.u32 %7, %7, %16;\n\t"
-            "addc.u32    %8, 0, 0;"
-            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]), "+r"(x[7]),
-              "=r"(c)
-            : "n"(F::M0), "n"(F::M1), "n"(F::M2), "n"(F::M3), "n"(F::M4), "n"(F::M5), "n"(F::M6), "n"(F::M7));
-        un_shr1<8>(x, c);
+    for (int i = 0; i < N; i++) {
+        const u64 s = (u64)q * m.v[i] + x[i] + c;
+        t[i] = (u32)s;
+        c = s >> 32;
+    }
+    t[N] = (u32)c;
+    if (k == 32) {
+#pragma unroll
+        for (int i = 0; i < N; i++) x[i] = t[i + 1];
     } else {
-        un_shr1<8>(x, 0);
+#pragma unroll
+        for (int i = 0; i < N; i++) x[i] = __funnelshift_r(t[i], t[i + 1], k);
     }
 }
 
+// Strip every trailing zero bit of w (nonzero), dividing x by 2 for each.
+template <class F>
+__device__ __forceinline__ void un_make_odd(u32 *w, u32 *x) {
+    constexpr int N = F::N;
+    while (w[0] == 0) {
+#pragma unroll
+        for (int i = 0; i < N - 1; i++) w[i] = w[i + 1];
+        w[N - 1] = 0;
+        fe_div2k<F>(x, 32);
+    }
+    const u32 k = __ffs(w[0]) - 1;
+    if (k) {
+#pragma unroll
+        for (int i = 0; i < N - 1; i++) w[i] = __funnelshift_r(w[i], w[i + 1], k);
+        w[N - 1] >>= k;
+        fe_div2k<F>(x, k);
+    }
+}
+
+// Invariants: x1 a = u and x2 a = v (mod N) up to the common power of two the
+// halvings divide out of both sides; u and v stay odd between steps, so every
+// step is one subtraction followed by all the halvings it makes possible.
+// The step bound keeps a non-canonical or non-invertible input from
+// looping: it yields zero.
 template <class F>
 __device__ __noinline__ Fe<F> fe_inv_binary(const Fe<F> &a_in, const Fe<F> &r3) {
     const Fe<F> a = fe_canon<F>(a_in);
@@ -916,32 +944,22 @@ __device__ __noinline__ Fe<F> fe_inv_binary(const Fe<F> &a_in, const Fe<F> &r3) 
         u[i] = a.l[i];
         v[i] = m.v[i];
     }
-    // One shift or one subtraction per step; a valid input (0 < a < N, N
-    // prime) needs at most ~4 * log2 N steps.  The zero check and the step
-    // bound keep a non-canonical input from looping: it yields zero.
-    bool done = false;
+    un_make_odd<F>(u, x1.l);  // v = N is odd
     for (int step = 0; step < 4096; step++) {
-        if (un_is_one<N>(u) || un_is_one<N>(v)) {
-            done = true;
-            break;
-        }
-        if (un_is_zero<N>(u) || un_is_zero<N>(v)) break;
-        if (!(u[0] & 1u)) {
-            un_shr1<N>(u, 0);
-            fe_half<F>(x1.l);
-        } else if (!(v[0] & 1u)) {
-            un_shr1<N>(v, 0);
-            fe_half<F>(x2.l);
-        } else if (un_geq<N>(u, v)) {
+        if (un_is_one<N>(u)) return fe_mul<F>(x1, r3);
+        if (un_is_one<N>(v)) return fe_mul<F>(x2, r3);
+        if (un_geq<N>(u, v)) {
             un_sub<N>(u, v);
+            if (un_is_zero<N>(u)) break;  // u == v > 1: no inverse
             x1 = fe_sub<F>(x1, x2);
+            un_make_odd<F>(u, x1.l);
         } else {
             un_sub<N>(v, u);
             x2 = fe_sub<F>(x2, x1);
+            un_make_odd<F>(v, x2.l);
         }
     }
-    if (!done) return fe_zero<F>();
-    return fe_mul<F>(un_is_one<N>(u) ? x1 : x2, r3);
+    return fe_zero<F>();
 }
 
 // 16-byte vector loads and stores (element addresses are 16-byte aligned).
@@ -1051,13 +1069,13 @@ template <class F, class MUL = MulInline>
 __device__ __forceinline__ XyzzT<F> xyzz_dbl(const XyzzT<F> &p) {
     if (xyzz_is_identity(p)) return p;
     Fe<F> u = fe_dbl(p.y);
-    Fe<F> v = MUL::mul(u, u);
+    Fe<F> v = MUL::sqr(u);
     Fe<F> w = MUL::mul(u, v);
     Fe<F> s = MUL::mul(p.x, v);
-    Fe<F> x2 = MUL::mul(p.x, p.x);
+    Fe<F> x2 = MUL::sqr(p.x);
     Fe<F> m = fe_add(fe_dbl(x2), x2);
     XyzzT<F> r;
-    r.x = fe_sub(fe_sub(MUL::mul(m, m), s), s);
+    r.x = fe_sub(fe_sub(MUL::sqr(m), s), s);
     r.y = fe_sub(MUL::mul(m, fe_sub(s, r.x)), MUL::mul(w, p.y));
     r.zz = MUL::mul(v, p.zz);
     r.zzz = MUL::mul(w, p.zzz);
@@ -1104,14 +1122,14 @@ __device__ __forceinline__ XyzzT<F> xyzz_add(const XyzzT<F> &p, const XyzzT<F> &
         if (fe_is_zero(R)) return xyzz_dbl<F, MUL>(p);
         return xyzz_identity<F>();
     }
-    Fe<F> pp = MUL::mul(P, P);
+    Fe<F> pp = MUL::sqr(P);
     Fe<F> ppp = MUL::mul(P, pp);
     Fe<F> Q = MUL::mul(u1, pp);
     XyzzT<F> r;
     r.zz = MUL::mul(MUL::mul(p.zz, q.zz), pp);
     r.zzz = MUL::mul(MUL::mul(p.zzz, q.zzz), ppp);
     Fe<F> t = MUL::mul(s1, ppp);
-    r.x = fe_sub(fe_sub(fe_sub(MUL::mul(R, R), ppp), Q), Q);
+    r.x = fe_sub(fe_sub(fe_sub(MUL::sqr(R), ppp), Q), Q);
     r.y = fe_sub(MUL::mul(R, fe_sub(Q, r.x)), t);
     return r;
 }
@@ -1130,7 +1148,7 @@ __device__ __forceinline__ AffineT<F> xyzz_to_affine_fast(const XyzzT<F> &p) {
     }
     Fe<F> a = fe_inv_binary<F>(p.zzz, fe_rcube<F>());
     Fe<F> zza = MUL::mul(p.zz, a);
-    Fe<F> b = MUL::mul(zza, zza);
+    Fe<F> b = MUL::sqr(zza);
     r.x = fe_canon(MUL::mul(p.x, b));
     r.y = fe_canon(MUL::mul(p.y, a));
     return r;

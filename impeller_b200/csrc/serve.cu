@@ -81,11 +81,7 @@ struct impeller_server {
     std::deque<u64> pending;
     std::unordered_map<u64, Job> jobs;
     std::vector<std::unique_ptr<Batch>> inflight;
-    // 2 x max_inflight slots: [0, max_inflight) on normal-priority streams,
-    // [max_inflight, 2 max_inflight) on the device's highest stream priority
-    // (batches holding a job of at least prio_points points; 0: unused)
     std::vector<cudaStream_t> streams;
-    u64 prio_points = 0;
     cudaMemPool_t pool = nullptr;  // batch scratch; keeps freed memory mapped for the next batch
     std::vector<u32 *> pinned;  // one result buffer per slot
     std::vector<void *> staging;  // one table-image buffer per slot
@@ -206,14 +202,9 @@ void dispatcher(impeller_server *s) {
                 s->pending.pop_front();
             }
             if (js.empty()) break;  // wait for memory to free
-            // a free slot of the batch's priority class: streams[k] is busy
-            // iff some in-flight batch uses it (at most max_inflight are, so
-            // each class always has a free one)
-            u64 largest = 0;
-            for (Job *j : js) largest = std::max(largest, j->n);
-            const bool high = s->prio_points && largest >= s->prio_points;
-            u32 slot = high ? s->max_inflight : 0;
-            for (const u32 end = slot + s->max_inflight; slot < end; slot++) {
+            // a free slot: streams[k] is busy iff some in-flight batch uses it
+            u32 slot = 0;
+            for (; slot < s->max_inflight; slot++) {
                 bool busy = false;
                 for (auto &p : s->inflight) busy |= p->stream == s->streams[slot];
                 if (!busy) break;
@@ -292,15 +283,11 @@ static cudaError_t server_setup(impeller_server *s) {
             return e;
         }
     }
-    int prio_least = 0, prio_greatest = 0;
-    if ((e = setup_step("stream priority range", cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest))) !=
-        cudaSuccess)
-        return e;
-    for (u32 i = 0; i < 2 * max_inflight; i++) {
+    for (u32 i = 0; i < max_inflight; i++) {
         cudaStream_t st;
         if ((e = injected(2, "stream")) != cudaSuccess) return e;
-        e = cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, i < max_inflight ? prio_least : prio_greatest);
-        if ((e = setup_step("stream", e)) != cudaSuccess) return e;
+        if ((e = setup_step("stream", cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking))) != cudaSuccess)
+            return e;
         s->streams.push_back(st);
         u32 *p = nullptr;
         if ((e = injected(3, "pinned result buffer")) != cudaSuccess) return e;
@@ -481,13 +468,6 @@ cudaError_t impeller_server_get_stats(impeller_server *s, impeller_server_stats 
         for (double v : l) sum += v;
         out->mean_ms = sum / (double)l.size();
     }
-    return cudaSuccess;
-}
-
-cudaError_t impeller_server_set_priority(impeller_server *s, uint64_t min_points) {
-    if (!s) return cudaErrorInvalidValue;
-    std::lock_guard<std::mutex> g(s->mu);
-    s->prio_points = min_points;
     return cudaSuccess;
 }
 

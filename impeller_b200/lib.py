@@ -87,7 +87,6 @@ SIGNATURES: dict[str, tuple] = {
     "impeller_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "impeller_server_inject_failures": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "impeller_server_fail_setup_step": (ctypes.c_int, [ctypes.c_uint32]),
-    "impeller_server_set_priority": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "impeller_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "impeller_gen_scalars": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                             ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),

@@ -503,11 +503,6 @@ class MsmServer:
         _lib.check(rc, "MSM job")
         return out, lat.value
 
-    def set_priority(self, min_points: int) -> None:
-        """Batches holding a job of at least min_points points run on
-        high-priority streams (0: off)."""
-        _lib.check(_lib.load().impeller_server_set_priority(self.handle, min_points), "set_priority")
-
     def inject_failures(self, batches: int) -> None:
         _lib.check(_lib.load().impeller_server_inject_failures(self.handle, batches), "inject")
 

@@ -227,12 +227,6 @@ cudaError_t impeller_server_inject_failures(impeller_server *s, uint32_t batches
  * with cudaErrorMemoryAllocation, releasing what it had made; the message of
  * impeller_last_error() names the step. */
 cudaError_t impeller_server_fail_setup_step(uint32_t step);
-/* Batches that hold a job of at least min_points points run on streams of
- * the device's highest priority, the rest on normal-priority streams (0, the
- * default: every batch at normal priority).  Large jobs then keep most of the
- * GPU while they run instead of sharing it evenly with every small job that
- * arrives meanwhile. */
-cudaError_t impeller_server_set_priority(impeller_server *s, uint64_t min_points);
 /* Drain queued and running jobs, then stop. */
 cudaError_t impeller_server_destroy(impeller_server *s);
 

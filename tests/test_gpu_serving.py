@@ -147,19 +147,3 @@ def test_server_setup_failure_releases_and_recovers(M, srs, step, what):
     srv.close()
     ctx.close()
 
-
-def test_priority_classes_keep_results(M, srs):
-    # large jobs on high-priority streams, small ones at normal priority:
-    # every result still equals the job run alone
-    ctx = M.MsmContext(srs)
-    srv = M.MsmServer(ctx, max_batch=4, max_inflight=4)
-    srv.set_priority(1 << 12)
-    rng = np.random.default_rng(9)
-    sizes = [int(2 ** rng.uniform(4, 15)) for _ in range(24)]
-    scal = [O.gen_scalars(n, seed=41, stream=i) for i, n in enumerate(sizes)]
-    ids = [srv.submit(s) for s in scal]
-    res = [srv.wait(j)[0] for j in ids]
-    srv.close()
-    for n, s, r in zip(sizes, scal, res):
-        assert (r == ctx.msm_host(s)).all(), n
-    ctx.close()
