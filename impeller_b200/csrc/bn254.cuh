@@ -117,6 +117,9 @@ struct Bn254 {
     using Fq = FqP;
     using Fr = FrP;
     static constexpr u32 PW = 16, XW = 32;
+    // signed-digit windows of width c (3 <= c <= 31) for scalars below r < 2^254:
+    // the top digit plus its incoming carry stays at most 2^(c-1)
+    __host__ __device__ static constexpr u32 windows(u32 c) { return (254u + c - 1u) / c; }
     static constexpr u32 GX[8] = {FqP::R0, FqP::R1, FqP::R2, FqP::R3, FqP::R4, FqP::R5, FqP::R6, FqP::R7};
     static constexpr u32 GY[8] = {0x8b1e1b3au, 0xa6ba871bu, 0xeb8e167bu, 0x14f1d651u,
                                   0xf0f28c58u, 0xccdd46deu, 0x340fbe5eu, 0x1c14ef83u};
@@ -125,6 +128,11 @@ struct Bls12381 {
     using Fq = BlsFqP;
     using Fr = BlsFrP;
     static constexpr u32 PW = 24, XW = 48;
+    // the smallest W with ((r - 1) >> (c (W - 1))) + 1 <= 2^(c - 1), r the
+    // group order (255 bits): ceil(255 / c), plus one for c = 3, 5, 15, 17
+    __host__ __device__ static constexpr u32 windows(u32 c) {
+        return c == 3 || c == 5 || c == 15 || c == 17 ? (255u + c - 1u) / c + 1u : (255u + c - 1u) / c;
+    }
     static constexpr u32 GX[12] = {0xfd530c16u, 0x5cb38790u, 0x9976fff5u, 0x7817fc67u, 0x143ba1c1u, 0x154f95c7u,
                                    0xf3d0e747u, 0xf0ae6acdu, 0x21dbf440u, 0xedce6eccu, 0x9e0bfb75u, 0x12017741u};
     static constexpr u32 GY[12] = {0x0ce72271u, 0xbaac93d5u, 0x7918fd8eu, 0x8c22631au, 0x570725ceu, 0xdd595f13u,

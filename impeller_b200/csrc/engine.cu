@@ -41,13 +41,8 @@ const char *last_error() { return g_err.c_str(); }
     } while (0)
 
 u32 digit_windows(u32 c, u32 curve) {
-    if (curve == CURVE_BLS12381) {
-        // smallest W with ((r - 1) >> (c (W - 1))) + 1 <= 2^(c - 1), r the BLS12-381 group order
-        static const u8 bls[32] = {0,  0,  0,  86, 64, 52, 43, 37, 32, 29, 26, 24, 22, 20, 19, 18,
-                                   16, 16, 15, 14, 13, 13, 12, 12, 11, 11, 10, 10, 10, 9,  9,  9};
-        return c < 32 ? bls[c] : 0;
-    }
-    return (254u + c - 1u) / c;
+    if (c < 3 || c > 31) return 0;
+    return curve == CURVE_BLS12381 ? Bls12381::windows(c) : Bn254::windows(c);
 }
 
 // Launch `kern` instantiated for the plan's curve.
@@ -528,8 +523,15 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
     }
 
     u32 *const buckets = bucket_out ? bucket_out : p.buckets;
-    AccumArgs aa{p.entries, p.offsets, nb, points, buckets, p.recb, p.recp, bucket_out ? 1u : 0u};
-    CURVE_LAUNCH(curve, k_accumulate, accum_blocks, accum_block, 0, st, aa);
+    AccumArgs aa{p.entries, p.offsets, nb, points, buckets, p.recb, p.recp};
+    if (bucket_out) {
+        if (curve == CURVE_BLS12381) k_accumulate<Bls12381, START_CARRY><<<accum_blocks, accum_block, 0, st>>>(aa);
+        else k_accumulate<Bn254, START_CARRY><<<accum_blocks, accum_block, 0, st>>>(aa);
+    } else if (curve == CURVE_BLS12381) {
+        k_accumulate<Bls12381, ACCUM_START_BLS><<<accum_blocks, accum_block, 0, st>>>(aa);
+    } else {
+        k_accumulate<Bn254, START_CONVERT><<<accum_blocks, accum_block, 0, st>>>(aa);
+    }
     CK_LAUNCH("k_accumulate");
     MARK(5);
 

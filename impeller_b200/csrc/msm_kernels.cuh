@@ -116,6 +116,48 @@ __device__ __forceinline__ void for_each_digit(const Fe<FR> &v, u32 c, u32 n_log
     step((u32)buf & mask, true);
 }
 
+// The same digits for a window width K known at compile time: the
+// bit-buffer routine with K and its window count W as constants, so that its
+// shifts, masks and loop trip counts fold (one 64-bit buffer live, as in the
+// runtime form; a fully positional extraction held every digit in registers
+// and spilled in the scatter kernel).
+template <u32 K, u32 W, class FR, class Emit>
+__device__ __forceinline__ void for_each_digit_fixed(const Fe<FR> &v, u32 n_windows, Emit &&emit) {
+    for_each_digit(v, K, W, n_windows, emit);
+}
+
+// Digits of one scalar of curve C: the constant-width form for the windows the
+// autotune table and the BLS12-381 window correction use, the bit-buffer
+// form otherwise.  c is uniform over a sort tile (one MSM per tile).
+template <class C, class Emit>
+__device__ __forceinline__ void digits_of(const Fe<typename C::Fr> &v, u32 c, u32 n_logical, u32 n_windows,
+                                          Emit &&emit) {
+    using FR = typename C::Fr;
+#ifndef IMPELLER_DIGITS_RUNTIME
+    switch (c) {
+#define IMPELLER_DIGITS_CASE(K)                                                        \
+    case K:                                                                            \
+        if (n_logical == C::windows(K)) {                                              \
+            for_each_digit_fixed<K, C::windows(K), FR>(v, n_windows, emit);            \
+            return;                                                                    \
+        }                                                                              \
+        break;
+        IMPELLER_DIGITS_CASE(8)
+        IMPELLER_DIGITS_CASE(10)
+        IMPELLER_DIGITS_CASE(13)
+        IMPELLER_DIGITS_CASE(15)
+        IMPELLER_DIGITS_CASE(16)
+        IMPELLER_DIGITS_CASE(17)
+        IMPELLER_DIGITS_CASE(18)
+        IMPELLER_DIGITS_CASE(20)
+#undef IMPELLER_DIGITS_CASE
+        default:
+            break;
+    }
+#endif
+    for_each_digit(v, c, n_logical, n_windows, emit);
+}
+
 // Lanes of a warp whose digits hit the same bucket share one atomic: heavy
 // buckets (the top window in a shared bucket set, the 0 / 1 / small scalars of
 // witness-like inputs) would otherwise serialize on a handful of addresses.
@@ -132,7 +174,7 @@ __global__ void k_histogram(const MsmDesc *__restrict__ descs, u32 *__restrict__
         const bool live = i < d.n;
         const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
                                           : fe_zero<typename C::Fr>();
-        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
+        digits_of<C>(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
             const u32 key = mag ? d.bucket_base + pw * B + mag - 1 : NONE;
             const u32 peers = __match_any_sync(0xffffffffu, key);
             if (key != NONE && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (u32)__popc(peers));
@@ -151,7 +193,7 @@ __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ c
         const bool live = i < d.n;
         const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
                                           : fe_zero<typename C::Fr>();
-        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
+        digits_of<C>(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
             const u32 key = mag ? d.bucket_base + pw * B + mag - 1 : NONE;
             const u32 peers = __match_any_sync(0xffffffffu, key);
             const u32 leader = __ffs(peers) - 1;
@@ -272,7 +314,7 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
         const bool live = i < end;
         const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
                                           : fe_zero<typename C::Fr>();
-        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
+        digits_of<C>(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
             if (mag) atomicAdd(&hist[(d.bucket_base + pw * B + mag - 1) >> FINE_BITS], 1u);
         });
     }
@@ -322,7 +364,7 @@ __global__ void __launch_bounds__(SORT_BLOCK, 2) k_coarse_scatter(SortArgs a) {
         const bool live = i < end;
         const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
                                           : fe_zero<typename C::Fr>();
-        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
+        digits_of<C>(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
             if (mag) {
                 const u32 key = d.bucket_base + pw * B + mag - 1;
                 const u32 slot = atomicAdd(&cur[key >> FINE_BITS], 1u);
@@ -589,7 +631,6 @@ struct AccumArgs {
     u32 *buckets;        // XYZZ, 32 u32 each, indexed by global bucket
     u32 *rec_bucket;     // 2 per thread
     u32 *rec_point;      // 2 per thread, XYZZ
-    u32 carry_in;        // 1: every bucket starts from its value in `buckets` (streamed chunks)
 };
 
 template <class C>
@@ -604,7 +645,7 @@ __device__ __forceinline__ AffineT<typename C::Fq> load_entry_point(const u32 *_
 // Otherwise the slice leaves a record: slot 2t for a piece that continues a
 // bucket begun in an earlier slice, slot 2t+1 for a piece whose bucket begins
 // in this slice and continues in later ones.
-// carry_in: the slice where a bucket begins starts it from the bucket's
+// START_CARRY: the slice where a bucket begins starts it from the bucket's
 // current value in `buckets` (a streamed call adds every chunk's points into
 // accumulators that persist across its chunks; buckets without entries in
 // the chunk are left as they are).
@@ -631,7 +672,17 @@ struct AccumShape {
     static constexpr u32 per_sm = C::XW == 32 ? ACCUM_BLOCKS_PER_SM : ACCUM_BLOCKS_PER_SM_BLS;
 };
 
-template <class C>
+// How a slice starts a bucket: START_CONVERT converts the first point (no
+// addition on that branch: 5 % fewer instructions per mixed addition on
+// BN254); START_IDENTITY adds every point, the first to the identity (one
+// addition code path: fewer registers); START_CARRY adds every point, the
+// first to the bucket's value in `buckets` (streamed chunks).
+enum : int { START_CONVERT = 0, START_IDENTITY = 1, START_CARRY = 2 };
+#ifndef ACCUM_START_BLS
+#define ACCUM_START_BLS START_CONVERT
+#endif
+
+template <class C, int START = START_CONVERT>
 __global__ void __launch_bounds__(AccumShape<C>::threads, AccumShape<C>::per_sm) k_accumulate(AccumArgs a) {
     using FQ = typename C::Fq;
     const u32 T = gridDim.x * blockDim.x;
@@ -666,13 +717,23 @@ __global__ void __launch_bounds__(AccumShape<C>::threads, AccumShape<C>::per_sm)
         // picks the value the addition starts from (lanes of a warp start
         // buckets at different entries, and a second inlined addition on
         // that branch would run divergently, doubling the loop's time).
-        if (fresh) {
-            acc = (a.carry_in && bbeg >= start) ? xyzz_load<FQ>(a.buckets + (size_t)b * C::XW) : xyzz_identity<FQ>();
-            fresh = false;
+        if constexpr (START != START_CONVERT) {
+            if (fresh) {
+                acc = (START == START_CARRY && bbeg >= start) ? xyzz_load<FQ>(a.buckets + (size_t)b * C::XW)
+                                                              : xyzz_identity<FQ>();
+                fresh = false;
+            }
+            acc = xyzz_add_affine(acc, q);
+            if (START == START_CARRY && pos + 2 == seg_end && seg_end == bend && b + 1 < a.nb)
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.buckets + (size_t)(b + 1) * C::XW));
+        } else {
+            if (fresh) {
+                acc = xyzz_from_affine(q);
+                fresh = false;
+            } else {
+                acc = xyzz_add_affine(acc, q);
+            }
         }
-        acc = xyzz_add_affine(acc, q);
-        if (a.carry_in && pos + 2 == seg_end && seg_end == bend && b + 1 < a.nb)
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(a.buckets + (size_t)(b + 1) * C::XW));
         if (pos + 1 == seg_end) {
             if (bbeg >= start && bend <= end) {
                 xyzz_store(a.buckets + (size_t)b * C::XW, acc);
