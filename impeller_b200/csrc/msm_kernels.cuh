@@ -116,48 +116,6 @@ __device__ __forceinline__ void for_each_digit(const Fe<FR> &v, u32 c, u32 n_log
     step((u32)buf & mask, true);
 }
 
-// The same digits for a window width K known at compile time: the
-// bit-buffer routine with K and its window count W as constants, so that its
-// shifts, masks and loop trip counts fold (one 64-bit buffer live, as in the
-// runtime form; a fully positional extraction held every digit in registers
-// and spilled in the scatter kernel).
-template <u32 K, u32 W, class FR, class Emit>
-__device__ __forceinline__ void for_each_digit_fixed(const Fe<FR> &v, u32 n_windows, Emit &&emit) {
-    for_each_digit(v, K, W, n_windows, emit);
-}
-
-// Digits of one scalar of curve C: the constant-width form for the windows the
-// autotune table and the BLS12-381 window correction use, the bit-buffer
-// form otherwise.  c is uniform over a sort tile (one MSM per tile).
-template <class C, class Emit>
-__device__ __forceinline__ void digits_of(const Fe<typename C::Fr> &v, u32 c, u32 n_logical, u32 n_windows,
-                                          Emit &&emit) {
-    using FR = typename C::Fr;
-#ifndef IMPELLER_DIGITS_RUNTIME
-    switch (c) {
-#define IMPELLER_DIGITS_CASE(K)                                                        \
-    case K:                                                                            \
-        if (n_logical == C::windows(K)) {                                              \
-            for_each_digit_fixed<K, C::windows(K), FR>(v, n_windows, emit);            \
-            return;                                                                    \
-        }                                                                              \
-        break;
-        IMPELLER_DIGITS_CASE(8)
-        IMPELLER_DIGITS_CASE(10)
-        IMPELLER_DIGITS_CASE(13)
-        IMPELLER_DIGITS_CASE(15)
-        IMPELLER_DIGITS_CASE(16)
-        IMPELLER_DIGITS_CASE(17)
-        IMPELLER_DIGITS_CASE(18)
-        IMPELLER_DIGITS_CASE(20)
-#undef IMPELLER_DIGITS_CASE
-        default:
-            break;
-    }
-#endif
-    for_each_digit(v, c, n_logical, n_windows, emit);
-}
-
 // Lanes of a warp whose digits hit the same bucket share one atomic: heavy
 // buckets (the top window in a shared bucket set, the 0 / 1 / small scalars of
 // witness-like inputs) would otherwise serialize on a handful of addresses.
@@ -174,7 +132,7 @@ __global__ void k_histogram(const MsmDesc *__restrict__ descs, u32 *__restrict__
         const bool live = i < d.n;
         const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
                                           : fe_zero<typename C::Fr>();
-        digits_of<C>(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
+        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
             const u32 key = mag ? d.bucket_base + pw * B + mag - 1 : NONE;
             const u32 peers = __match_any_sync(0xffffffffu, key);
             if (key != NONE && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (u32)__popc(peers));
@@ -193,7 +151,7 @@ __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ c
         const bool live = i < d.n;
         const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
                                           : fe_zero<typename C::Fr>();
-        digits_of<C>(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
+        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
             const u32 key = mag ? d.bucket_base + pw * B + mag - 1 : NONE;
             const u32 peers = __match_any_sync(0xffffffffu, key);
             const u32 leader = __ffs(peers) - 1;
@@ -314,7 +272,7 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
         const bool live = i < end;
         const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
                                           : fe_zero<typename C::Fr>();
-        digits_of<C>(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
+        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
             if (mag) atomicAdd(&hist[(d.bucket_base + pw * B + mag - 1) >> FINE_BITS], 1u);
         });
     }
@@ -364,7 +322,7 @@ __global__ void __launch_bounds__(SORT_BLOCK, 2) k_coarse_scatter(SortArgs a) {
         const bool live = i < end;
         const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
                                           : fe_zero<typename C::Fr>();
-        digits_of<C>(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
+        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
             if (mag) {
                 const u32 key = d.bucket_base + pw * B + mag - 1;
                 const u32 slot = atomicAdd(&cur[key >> FINE_BITS], 1u);
@@ -678,8 +636,10 @@ struct AccumShape {
 // addition code path: fewer registers); START_CARRY adds every point, the
 // first to the bucket's value in `buckets` (streamed chunks).
 enum : int { START_CONVERT = 0, START_IDENTITY = 1, START_CARRY = 2 };
+// BLS12-381 (measured at 2^22, tables c = 20): identity start 22.50 ms per
+// MSM, convert 22.61 ms (its two code paths spill 44 bytes at 168 registers).
 #ifndef ACCUM_START_BLS
-#define ACCUM_START_BLS START_CONVERT
+#define ACCUM_START_BLS START_IDENTITY
 #endif
 
 template <class C, int START = START_CONVERT>
@@ -1040,22 +1000,32 @@ __global__ void __launch_bounds__(TREE_BLOCK, C::XW == 32 ? 2 : 1) k_reduce_tree
         A = xyzz_load<FQ>(a.parts_v + (size_t)(gr.in_base + lane) * C::XW);
         x = xyzz_load<FQ>(a.parts_s + (size_t)(gr.in_base + lane) * C::XW);
     }
+    // Lanes at or above in_count hold the identity; P, the next power of two
+    // at or above in_count, bounds every step below (a window's last group
+    // is often small).
+    u32 P = 1;
+    while (P < gr.in_count) P <<= 1;
     // inclusive suffix sums of S
 #pragma unroll 1
-    for (u32 o = 1; o < 32; o <<= 1) {
+    for (u32 o = 1; o < P; o <<= 1) {
         Xz y = xyzz_shfl_down(x, o);
         if (lane + o < 32) x = xyzz_add<FQ, TailMul>(x, y);
     }
     Xz w = lane ? x : xyzz_identity<FQ>();
-    // The sums of A and of w over the warp: the first step folds lanes l and
-    // l + 16 so that lanes 0-15 carry partial sums of A and lanes 16-31 of w,
-    // then each half reduces on its own -- one addition per step, not two.
-    Xz v = xyzz_add<FQ, TailMul>(lane < 16 ? A : w, xyzz_shfl_xor(lane < 16 ? w : A, 16));
+    // The sums of A and of w over the group: the first step folds lanes l
+    // and l + P/2 so that lanes below P/2 carry partial sums of A and lanes
+    // P/2 .. P-1 of w, then each half reduces on its own -- one addition per
+    // step, not two.  Lane 0 ends with the sum of A, lane P/2 with that of w.
+    const u32 half = P >> 1;
+    Xz v = A;
+    if (half) {
+        v = xyzz_add<FQ, TailMul>(lane < half ? A : w, xyzz_shfl_xor(lane < half ? w : A, half));
 #pragma unroll 1
-    for (u32 o = 8; o; o >>= 1) v = xyzz_add<FQ, TailMul>(v, xyzz_shfl_xor(v, o));
-    if (lane == 16)
+        for (u32 o = half >> 1; o; o >>= 1) v = xyzz_add<FQ, TailMul>(v, xyzz_shfl_xor(v, o));
+    }
+    if (lane == half && half)
         for (u32 k = 0; k < gr.shift; k++) v = xyzz_dbl<FQ, TailMul>(v);
-    w = xyzz_shfl_down(v, 16);
+    w = half ? xyzz_shfl_down(v, half) : xyzz_identity<FQ>();
     if (lane == 0) {
         A = xyzz_add<FQ, TailMul>(v, w);
         if (gr.out & TREE_FINAL) {
