@@ -129,7 +129,8 @@ __device__ Fe<F> test_op(int op, const Fe<F> &a, const Fe<F> &b) {
     case 6: return fe_from_mont<F>(a);
     case 7: return fe_inv<F>(a);
     case 8: return fe_pow<F>(a, b.l);
-    default: return fe_inv_binary<F>(a, fe_mul<F>(fe_mul<F>(r2, r2), fe_one<F>()));
+    case 9: return fe_inv_binary<F>(a, fe_mul<F>(fe_mul<F>(r2, r2), fe_one<F>()));
+    default: return fe_inv_divsteps<F>(a, fe_mul<F>(fe_mul<F>(r2, r2), fe_one<F>()));
     }
 }
 
@@ -338,7 +339,7 @@ cudaError_t impeller_op_latency(int op, uint32_t iters, double *cycles_per_op) {
 
 cudaError_t impeller_test_field_op(int field, int op, const uint32_t *d_a, const uint32_t *d_b, uint32_t *d_out,
                                    uint64_t count, cudaStream_t s) {
-    if (field < 0 || field > 3 || op < 0 || op > 9 || !d_a || !d_out) {
+    if (field < 0 || field > 3 || op < 0 || op > 10 || !d_a || !d_out) {
         impeller::set_error("impeller_test_field_op: bad argument");
         return cudaErrorInvalidValue;
     }

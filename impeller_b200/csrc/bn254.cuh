@@ -218,6 +218,7 @@ __device__ __forceinline__ bool fe_is_zero(const Fe<F> &a) {
 }  // namespace ec
 
 #include "field12.cuh"
+#include "safegcd.cuh"
 
 namespace ec {
 
@@ -970,6 +971,19 @@ __device__ __noinline__ Fe<F> fe_inv_binary(const Fe<F> &a_in, const Fe<F> &r3) 
     return fe_zero<F>();
 }
 
+// The same inversion by Bernstein-Yang divsteps (safegcd.cuh): batches of 30
+// divsteps on the low words, one full-width update per batch; 3-4x fewer
+// dependent instructions than the binary method for 254- and 381-bit moduli.
+// One Montgomery product with R^3 turns A^-1 R^-1 into A^-1 R as above.
+template <class F>
+__device__ __noinline__ Fe<F> fe_inv_divsteps(const Fe<F> &a_in, const Fe<F> &r3) {
+    const Fe<F> a = fe_canon<F>(a_in);
+    constexpr Words<F::N> m = words(F::M);
+    Fe<F> r;
+    sg::inverse<F::N>(a.l, m.v, r.l);
+    return fe_mul<F>(r, r3);
+}
+
 // 16-byte vector loads and stores (element addresses are 16-byte aligned).
 template <class F>
 __device__ __forceinline__ Fe<F> fe_load(const u32 *p) {
@@ -1144,7 +1158,7 @@ __device__ __forceinline__ XyzzT<F> xyzz_add(const XyzzT<F> &p, const XyzzT<F> &
 
 __device__ __forceinline__ Fq fq_r3() { return fe_rcube<FqP>(); }
 
-// Canonical affine form; identity -> (0, 0).  Latency-optimised (binary
+// Canonical affine form; identity -> (0, 0).  Latency-optimised (divstep
 // inversion): used once per MSM result.
 template <class F, class MUL = MulInline>
 __device__ __forceinline__ AffineT<F> xyzz_to_affine_fast(const XyzzT<F> &p) {
@@ -1154,7 +1168,7 @@ __device__ __forceinline__ AffineT<F> xyzz_to_affine_fast(const XyzzT<F> &p) {
         r.y = fe_zero<F>();
         return r;
     }
-    Fe<F> a = fe_inv_binary<F>(p.zzz, fe_rcube<F>());
+    Fe<F> a = fe_inv_divsteps<F>(p.zzz, fe_rcube<F>());
     Fe<F> zza = MUL::mul(p.zz, a);
     Fe<F> b = MUL::sqr(zza);
     r.x = fe_canon(MUL::mul(p.x, b));

@@ -248,7 +248,8 @@ cudaError_t impeller_gen_points_curve(int curve, uint32_t *d_out, uint64_t n, ui
 /* Element-wise field / point operations on the device, for parity tests.
  * field: 0 = BN254 Fq, 1 = BN254 Fr, 2 = BLS12-381 Fq (12 u32 per element),
  * 3 = BLS12-381 Fr.  op: 0 add, 1 sub, 2 mul, 3 sqr, 4 neg, 5 to_mont,
- * 6 from_mont, 7 inv (Fermat), 8 pow, 9 inv (binary extended Euclid).  Point ops (affine in/out): 0 add (madd path),
+ * 6 from_mont, 7 inv (Fermat), 8 pow, 9 inv (binary extended Euclid), 10 inv
+ * (Bernstein-Yang divsteps, the one MSM results use).  Point ops (affine in/out): 0 add (madd path),
  * 1 dbl, 2 add via XYZZ+XYZZ, 3 k*P (k plain 256-bit). */
 cudaError_t impeller_test_field_op(int field, int op, const uint32_t *d_a, const uint32_t *d_b, uint32_t *d_out,
                                    uint64_t count, cudaStream_t s);

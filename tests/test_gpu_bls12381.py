@@ -96,6 +96,7 @@ def test_field_ops_match_oracle(M, field, modulus, words):
     want = O.field_op(field, O.INV, a[:64])
     assert (field_op_gpu(M, field, O.INV, a[:64]) == want).all()
     assert (field_op_gpu(M, field, 9, a[:64]) == want).all()  # binary extended Euclid
+    assert (field_op_gpu(M, field, 10, a[:64]) == want).all()  # Bernstein-Yang divsteps
     e = random_elems(rng, 32, modulus, words)
     want = O.field_op(field, O.POW, a[:32], e)
     assert (field_op_gpu(M, field, O.POW, a[:32], e) == want).all()

@@ -75,6 +75,7 @@ def test_field_ops_match_oracle(M, field, modulus):
     want = O.field_op(field, O.INV, a[:64])
     assert (field_op_gpu(M, field, O.INV, a[:64]) == want).all()
     assert (field_op_gpu(M, field, 9, a[:64]) == want).all()  # binary extended Euclid
+    assert (field_op_gpu(M, field, 10, a[:64]) == want).all()  # Bernstein-Yang divsteps
     want = O.field_op(field, O.POW, a[:32], b[:32])
     assert (field_op_gpu(M, field, O.POW, a[:32], b[:32]) == want).all()
 
