@@ -857,7 +857,7 @@ __global__ void __launch_bounds__(REDUCE_BLOCK, C::XW == 32 ? REDUCE_BLOCKS_PER_
     }
     Xz ex = xyzz_shfl_down(x, 1);
     if (lane == 31) ex = xyzz_identity<FQ>();
-    for (u32 k = 0, lg = ilog2(wd.chunk); k < lg; k++) ex = xyzz_dbl<FQ, ReduceMul>(ex);
+    ex = xyzz_dbl_n<FQ, ReduceMul>(ex, ilog2(wd.chunk));
     Xz v = xyzz_add<FQ, ReduceMul>(sos, ex);
 #pragma unroll 1
     for (u32 o = 16; o; o >>= 1) v = xyzz_add<FQ, ReduceMul>(v, xyzz_shfl_down(v, o));
@@ -928,7 +928,7 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
     Xz ex = xyzz_shfl_down(x, 1);
     if (lane == 31) ex = xyzz_identity<FQ>();
     ex = xyzz_add<FQ, ReduceMul>(ex, later);
-    for (u32 k = 0, lg = ilog2(g); k < lg; k++) ex = xyzz_dbl<FQ, ReduceMul>(ex);
+    ex = xyzz_dbl_n<FQ, ReduceMul>(ex, ilog2(g));
     Xz rs = xyzz_add<FQ, ReduceMul>(sos, ex);  // this group's share of sum_w w * S_w
 #pragma unroll 1
     for (u32 o = 16; o; o >>= 1) {
@@ -951,7 +951,7 @@ __global__ void __launch_bounds__(WSUM_BLOCK) k_window_sum(WindowSumArgs a) {
         }
         if (lane == 0) {
             const u32 shift = ilog2(wd.chunk) + 5;  // 32 lanes per warp partial
-            for (u32 k = 0; k < shift; k++) r2 = xyzz_dbl<FQ, ReduceMul>(r2);
+            r2 = xyzz_dbl_n<FQ, ReduceMul>(r2, shift);
             xyzz_store(a.wres + (size_t)win * C::XW, xyzz_add<FQ, ReduceMul>(v2, r2));
         }
     }
@@ -1023,8 +1023,7 @@ __global__ void __launch_bounds__(TREE_BLOCK, C::XW == 32 ? 2 : 1) k_reduce_tree
 #pragma unroll 1
         for (u32 o = half >> 1; o; o >>= 1) v = xyzz_add<FQ, TailMul>(v, xyzz_shfl_xor(v, o));
     }
-    if (lane == half && half)
-        for (u32 k = 0; k < gr.shift; k++) v = xyzz_dbl<FQ, TailMul>(v);
+    if (lane == half && half) v = xyzz_dbl_n<FQ, TailMul>(v, gr.shift);
     w = half ? xyzz_shfl_down(v, half) : xyzz_identity<FQ>();
     if (lane == 0) {
         A = xyzz_add<FQ, TailMul>(v, w);
@@ -1047,7 +1046,8 @@ struct FinalArgs {
 };
 
 // One thread per MSM: Horner over its windows, sum_w 2^(c w) T_w with
-// c * (windows - 1) doublings, then the carry and the affine form.
+// c * (windows - 1) doublings (in Jacobian form between the additions),
+// then the carry and the affine form.
 template <class C>
 __global__ void k_final(FinalArgs f) {
     using FQ = typename C::Fq;
@@ -1056,8 +1056,7 @@ __global__ void k_final(FinalArgs f) {
     const MsmDesc d = f.descs[m];
     XyzzT<FQ> acc = xyzz_identity<FQ>();
     for (int w = (int)d.n_windows - 1; w >= 0; w--) {
-        if (!xyzz_is_identity(acc))
-            for (u32 k = 0; k < d.c; k++) acc = xyzz_dbl<FQ, FinalMul>(acc);
+        acc = xyzz_dbl_n<FQ, FinalMul>(acc, d.c);
         acc = xyzz_add<FQ, FinalMul>(acc, xyzz_load<FQ>(f.wres + (size_t)(d.win_base + w) * C::XW));
     }
     if (f.carry) acc = xyzz_add<FQ, FinalMul>(acc, xyzz_load<FQ>(f.carry + (size_t)m * C::XW));
