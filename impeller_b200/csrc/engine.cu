@@ -141,6 +141,7 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
         d.bucket_base = (u32)nb;
         d.win_base = (u32)wins.size();
         d.table_base = s.table_base;
+        d.entry_base = (u32)entries;
         for (u32 pw = 0; pw < nw; pw++) {
             WinDesc w{};
             w.bucket_base = (u32)(nb + pw * B);
@@ -469,7 +470,7 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
                     reinterpret_cast<unsigned short *>(sb + layout.o_cfine),
                     reinterpret_cast<uint4 *>(sb + layout.o_segs), reinterpret_cast<uint2 *>(sb + layout.o_binseg),
                     reinterpret_cast<u32 *>(sb + layout.o_nsegs), reinterpret_cast<u32 *>(sb + layout.o_seghist),
-                    reinterpret_cast<u32 *>(sb + layout.o_segcur), p.offsets, p.entries};
+                    reinterpret_cast<u32 *>(sb + layout.o_segcur), p.offsets, p.entries, p.entries};
         // the scan padding of the tile counts and the long-run counter of the fixups
         k_zero_words<<<1, 256, 0, st>>>(cnt + ncnt, cnt_pad - ncnt, p.longl, 1);
         CK_LAUNCH("k_zero_words");

@@ -53,6 +53,7 @@ struct MsmDesc {
     u32 bucket_base;     // global index of bucket (window 0, weight 1)
     u32 win_base;        // global index of physical window 0
     u32 table_base;      // index of this MSM's table 0 in the point array
+    u32 entry_base;      // first digit slot of this MSM (sum of n * n_logical of the earlier MSMs)
 };
 
 // One physical window of one MSM (bucket reduction unit).
@@ -215,6 +216,8 @@ struct SortArgs {
     u32 *segcur;            // segcap x FINE: each segment's first slot per bucket
     u32 *offsets;           // nb + 1 (output)
     u32 *entries;           // (output)
+    u32 *keys;              // per MSM, tile and digit window: the digit's bucket (bit 31: sign) or NONE;
+                            // written by k_coarse_count, read by k_coarse_scatter (may alias entries)
 };
 
 // Exclusive scan over the block (blockDim a multiple of 32, at most 1024).
@@ -267,13 +270,24 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
     for (u32 b = threadIdx.x; b < a.nbins; b += blockDim.x) hist[b] = 0;
     __syncthreads();
     const u32 B = 1u << (d.c - 1);
+    // the tile's keys, window-major: key of window w, scalar i at w * (end - start) + i - start
+    const u32 tile_n = end - start;
+    u32 *kp = a.keys + d.entry_base + (size_t)start * d.n_logical;
     for (u32 base = start; base < end; base += blockDim.x) {
         const u32 i = base + threadIdx.x;
         const bool live = i < end;
         const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
                                           : fe_zero<typename C::Fr>();
-        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32) {
-            if (mag) atomicAdd(&hist[(d.bucket_base + pw * B + mag - 1) >> FINE_BITS], 1u);
+        u32 *kw = kp + (i - start);
+        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32, u32 mag, u32 sign) {
+            u32 key = NONE;
+            if (mag) {
+                key = d.bucket_base + pw * B + mag - 1;
+                atomicAdd(&hist[key >> FINE_BITS], 1u);
+                key |= sign << 31;
+            }
+            if (live) *kw = key;
+            kw += tile_n;
         });
     }
     __syncthreads();
@@ -317,19 +331,26 @@ __global__ void __launch_bounds__(SORT_BLOCK, 2) k_coarse_scatter(SortArgs a) {
         }
     }
     __syncthreads();
-    for (u32 base = start; base < end; base += blockDim.x) {
-        const u32 i = base + threadIdx.x;
-        const bool live = i < end;
-        const Fe<typename C::Fr> v = live ? fe_from_mont<typename C::Fr>(fe_load<typename C::Fr>(d.scalars + 8ull * i))
-                                          : fe_zero<typename C::Fr>();
-        for_each_digit(v, d.c, d.n_logical, d.n_windows, [&](u32 pw, u32 table, u32 mag, u32 sign) {
-            if (mag) {
-                const u32 key = d.bucket_base + pw * B + mag - 1;
-                const u32 slot = atomicAdd(&cur[key >> FINE_BITS], 1u);
-                stage_e[slot] = ((d.table_base + table * d.table_stride + i) << 1) | sign;
-                stage_f[slot] = (unsigned short)(key & (FINE - 1u));
+    // the keys k_coarse_count left for this tile (window-major)
+    const u32 tile_n = end - start, nsets = d.n_windows;
+    const u32 *kp = a.keys + d.entry_base + (size_t)start * d.n_logical;
+    for (u32 i = start + threadIdx.x; i < end; i += blockDim.x) {
+        const u32 *kw = kp + (i - start);
+        u32 pw = 0, table = 0;
+#pragma unroll 4
+        for (u32 w = 0; w < d.n_logical; w++) {
+            const u32 key = kw[(size_t)w * tile_n];
+            if (key != NONE) {
+                const u32 bk = key & 0x7fffffffu;
+                const u32 slot = atomicAdd(&cur[bk >> FINE_BITS], 1u);
+                stage_e[slot] = ((d.table_base + table * d.table_stride + i) << 1) | (key >> 31);
+                stage_f[slot] = (unsigned short)(bk & (FINE - 1u));
             }
-        });
+            if (++pw == nsets) {
+                pw = 0;
+                table++;
+            }
+        }
     }
     __syncthreads();
     // one warp per bin writes the bin's run of this tile: one coalesced run

@@ -129,6 +129,7 @@ __global__ void k_noalloc_tables(unsigned char *base, const u32 *scalars, u32 n)
         d->bucket_base = 0;
         d->win_base = 0;
         d->table_base = 0;
+        d->entry_base = 0;
     }
     for (u32 i = t; i < W; i += blockDim.x) {
         WinDesc x;
