@@ -334,21 +334,28 @@ __global__ void __launch_bounds__(SORT_BLOCK, 2) k_coarse_scatter(SortArgs a) {
     // the keys k_coarse_count left for this tile (window-major)
     const u32 tile_n = end - start, nsets = d.n_windows;
     const u32 *kp = a.keys + d.entry_base + (size_t)start * d.n_logical;
+    // Eight keys are loaded before any is placed, so that their load
+    // latencies overlap (the kernel is otherwise bound by them).
+    constexpr u32 KB = 8;
     for (u32 i = start + threadIdx.x; i < end; i += blockDim.x) {
         const u32 *kw = kp + (i - start);
         u32 pw = 0, table = 0;
-#pragma unroll 4
-        for (u32 w = 0; w < d.n_logical; w++) {
-            const u32 key = kw[(size_t)w * tile_n];
-            if (key != NONE) {
-                const u32 bk = key & 0x7fffffffu;
-                const u32 slot = atomicAdd(&cur[bk >> FINE_BITS], 1u);
-                stage_e[slot] = ((d.table_base + table * d.table_stride + i) << 1) | (key >> 31);
-                stage_f[slot] = (unsigned short)(bk & (FINE - 1u));
-            }
-            if (++pw == nsets) {
-                pw = 0;
-                table++;
+        for (u32 w0 = 0; w0 < d.n_logical; w0 += KB) {
+            u32 key[KB];
+#pragma unroll
+            for (u32 j = 0; j < KB; j++) key[j] = w0 + j < d.n_logical ? __ldg(kw + (size_t)(w0 + j) * tile_n) : NONE;
+#pragma unroll
+            for (u32 j = 0; j < KB; j++) {
+                if (key[j] != NONE) {
+                    const u32 bk = key[j] & 0x7fffffffu;
+                    const u32 slot = atomicAdd(&cur[bk >> FINE_BITS], 1u);
+                    stage_e[slot] = ((d.table_base + table * d.table_stride + i) << 1) | (key[j] >> 31);
+                    stage_f[slot] = (unsigned short)(bk & (FINE - 1u));
+                }
+                if (++pw == nsets) {
+                    pw = 0;
+                    table++;
+                }
             }
         }
     }
