@@ -402,6 +402,17 @@ cudaError_t run_card(CardJob &J) {
                 const u64 mk = bounds[k + 1] - s0;
                 const u32 slot = staged ? k % PART_STAGES : 0;
                 if (staged && k >= PART_STAGES) CK(cudaStreamWaitEvent(cs, computed[k - PART_STAGES], 0));
+                // the chunk's scalars first: its sort needs only them and runs
+                // while its points are still being copied
+                for (u32 b = 0; b < M; b++) {
+                    u32 *dst = staged ? d_scalars + slot * scalar_stage + (size_t)b * part_len * 8
+                                      : d_scalars + (size_t)b * part_len * 8 + s0 * 8;
+                    CK(cudaMemcpyAsync(dst, J.h_scalars[g + b] + (J.L.card_off + s0) * 8, mk * 32,
+                                       cudaMemcpyHostToDevice, cs));
+                }
+                cudaEvent_t scalars_landed = events.get();
+                if (!scalars_landed) return cudaErrorUnknown;
+                CK(cudaEventRecord(scalars_landed, cs));
                 // points of this chunk: staged -> its stage buffer; resident -> in place
                 u32 *pbase = staged ? d_points + slot * point_stage : d_points + s0 * PW;
                 if (!points_resident)
@@ -409,20 +420,15 @@ cudaError_t run_card(CardJob &J) {
                         CK(cudaMemcpyAsync(pbase + (size_t)t * part_len * PW,
                                            J.h_points[t] + (J.L.card_off + s0) * PW, mk * PW * 4,
                                            cudaMemcpyHostToDevice, cs));
-                for (u32 b = 0; b < M; b++) {
-                    u32 *dst = staged ? d_scalars + slot * scalar_stage + (size_t)b * part_len * 8
-                                      : d_scalars + (size_t)b * part_len * 8 + s0 * 8;
-                    CK(cudaMemcpyAsync(dst, J.h_scalars[g + b] + (J.L.card_off + s0) * 8, mk * 32,
-                                       cudaMemcpyHostToDevice, cs));
-                }
                 cudaEvent_t landed = events.get();
                 if (!landed) return cudaErrorUnknown;
                 CK(cudaEventRecord(landed, cs));
                 if (cfg.debug) cudaEventRecord(tl[3 * k], cs);
-                CK(cudaStreamWaitEvent(st, landed, 0));
+                CK(cudaStreamWaitEvent(st, scalars_landed, 0));
                 if (cfg.debug) cudaEventRecord(tl[3 * k + 1], st);
                 plan = chunk_plan[k];
-                cudaError_t e = plan->launch_chunk(plan_scratch, pbase, d_acc, k == 0, st, d_images + k * J.L.image_cap);
+                cudaError_t e = plan->launch_chunk(plan_scratch, pbase, d_acc, k == 0, st, d_images + k * J.L.image_cap,
+                                                   landed);
                 if (e != cudaSuccess) return e;
                 if (cfg.debug) cudaEventRecord(tl[3 * k + 2], st);
                 if (staged) {

@@ -449,7 +449,7 @@ __global__ void k_zero_words(u32 *__restrict__ p, u32 n, u32 *__restrict__ q, u3
 // when d_image is given, so nothing here queues behind transfers on a copy
 // engine.
 cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, bool record_staged,
-                            const void *d_image, u32 *bucket_out) {
+                            const void *d_image, u32 *bucket_out, cudaEvent_t points_ready) {
     const PlanPtrs p = plan_ptrs(layout, desc_off, win_off, blk_off, tf_off, scratch, nullptr, nullptr, d_image);
     cudaError_t pe;
     MARK(0);
@@ -523,6 +523,7 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
         MARK(4);
     }
 
+    if (points_ready) CK(cudaStreamWaitEvent(st, points_ready, 0));
     u32 *const buckets = bucket_out ? bucket_out : p.buckets;
     AccumArgs aa{p.entries, p.offsets, nb, points, buckets, p.recb, p.recp};
     if (bucket_out) {
@@ -591,7 +592,7 @@ void Plan::write_image(void *dst, const u32 *const *scalars) const {
 }
 
 cudaError_t Plan::launch_chunk(void *scratch, const u32 *points, u32 *acc, bool first, cudaStream_t st,
-                               const void *d_image) {
+                               const void *d_image, cudaEvent_t points_ready) {
     if (first) {
         // every accumulator starts as the identity (all-zero XYZZ)
         const u64 words = (u64)nb * xyzz_words(curve);
@@ -603,7 +604,7 @@ cudaError_t Plan::launch_chunk(void *scratch, const u32 *points, u32 *acc, bool 
             acc, (u32)words, nullptr, 0);
         CK_LAUNCH("k_zero_words");
     }
-    return run_front(scratch, points, st, true, d_image, acc);
+    return run_front(scratch, points, st, true, d_image, acc, points_ready);
 }
 
 cudaError_t Plan::launch_chunked_tail(void *scratch, const u32 *acc, u32 *results, int carry_mode, cudaStream_t st,

@@ -103,8 +103,11 @@ class Plan {
     // have the same window structure (same c, windows and MSM count).
     // d_image: the chunk's table image (write_image) already on the device;
     // null = stage() before and upload on the stream as launch does.
+    // points_ready: when given, the stream waits for it after the sort and
+    // before the accumulation (the sort reads only the scalars, so it can run
+    // while the chunk's points are still being copied).
     cudaError_t launch_chunk(void *scratch, const u32 *points, u32 *acc, bool first, cudaStream_t stream,
-                             const void *d_image = nullptr);
+                             const void *d_image = nullptr, cudaEvent_t points_ready = nullptr);
     cudaError_t launch_chunked_tail(void *scratch, const u32 *acc, u32 *results, int carry_mode,
                                     cudaStream_t stream, u32 *carry_ext = nullptr, const void *d_image = nullptr);
     size_t acc_bytes() const { return (size_t)nb * xyzz_words(curve) * 4; }
@@ -147,7 +150,7 @@ class Plan {
     // bucket_out: accumulate into these buckets, each starting from its
     // current value (streamed chunks); null = the plan's own buckets, fresh.
     cudaError_t run_front(void *scratch, const u32 *points, cudaStream_t stream, bool record_staged,
-                          const void *d_image, u32 *bucket_out = nullptr);
+                          const void *d_image, u32 *bucket_out = nullptr, cudaEvent_t points_ready = nullptr);
     cudaError_t run_tail(void *scratch, const u32 *buckets, bool dense, u32 *results, int carry_mode,
                          cudaStream_t stream, u32 *carry_ext, const void *d_image);
 
