@@ -68,24 +68,32 @@ int sm_count(int device) {
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// The sort-path rule of Plan::build, from the shapes alone: bins of FINE
-// buckets (at most SORT_MAX_BINS) times tiles of scalars (sized by the most
-// digit windows of any MSM) at most SORT_MAX_CELLS count cells.
+// The sort-path rule of Plan::build, from the shapes alone.  Each MSM's
+// buckets start on a multiple of FINE, so every coarse bin belongs to one
+// MSM, and the count matrix holds, per MSM, its bins times its tiles of
+// scalars (tiles sized by the most digit windows of any MSM): at most
+// SORT_MAX_BINS bins and SORT_MAX_CELLS count cells.
 bool Plan::two_level_sort(const std::vector<MsmShape> &shapes) {
     u64 nb = 0;
     u32 wmax = 1;
     for (const MsmShape &s : shapes) {
         if (s.c < 3 || s.c > 31) return false;
-        const u32 W = digit_windows(s.c, s.curve);
-        const u32 nw = (s.n_windows == 0 || s.n_windows > W) ? W : s.n_windows;
-        nb += (u64)nw << (s.c - 1);
-        wmax = std::max(wmax, W);
+        wmax = std::max(wmax, digit_windows(s.c, s.curve));
     }
     const u32 tile = std::max(32u, std::min(1024u, (STAGE_ENTRIES / wmax) & ~31u));
-    u64 stiles = 0;
-    for (const MsmShape &s : shapes) stiles += (s.n + tile - 1) / tile;
+    u64 stiles = 0, cells = 0;
+    for (const MsmShape &s : shapes) {
+        const u32 W = digit_windows(s.c, s.curve);
+        const u32 nw = (s.n_windows == 0 || s.n_windows > W) ? W : s.n_windows;
+        nb = align_up(nb, FINE);
+        const u64 b0 = nb / FINE;
+        nb += (u64)nw << (s.c - 1);
+        const u64 tiles = (s.n + tile - 1) / tile;
+        stiles += tiles;
+        cells += ((nb + FINE - 1) / FINE - b0) * tiles;
+    }
     const u64 nbins = (nb + FINE - 1) / FINE;
-    return stiles > 0 && nbins <= SORT_MAX_BINS && nbins * stiles <= SORT_MAX_CELLS;
+    return stiles > 0 && nbins <= SORT_MAX_BINS && cells <= SORT_MAX_CELLS;
 }
 
 bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
@@ -131,6 +139,7 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
             set_error("point index space (tables x length) exceeds 2^31");
             return false;
         }
+        nb = align_up(nb, FINE);  // every coarse bin of the sort belongs to one MSM
         MsmDesc &d = descs[m];
         d.scalars = nullptr;
         d.n = s.n;
@@ -246,11 +255,29 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     }
     tile_first[p.M] = (u32)stiles;
     const u64 nbins = (nb + FINE - 1) / FINE;
-    p.msd = stiles > 0 && nbins <= SORT_MAX_BINS && nbins * stiles <= SORT_MAX_CELLS;
+    // count cells: per MSM, its bins x its tiles; bin_cell[b] = first cell of bin b
+    std::vector<u32> bin_cell;
+    u64 cells = 0;
+    if (nbins <= SORT_MAX_BINS) {
+        bin_cell.assign(nbins + 1, 0);
+        for (u32 m = 0; m < p.M; m++) {
+            const MsmDesc &d = descs[m];
+            const u64 blo = d.bucket_base / FINE;
+            const u64 bhi = ((u64)d.bucket_base + ((u64)d.n_windows << (d.c - 1)) - 1) / FINE;
+            const u64 tiles = tile_first[m + 1] - tile_first[m];
+            for (u64 b = blo; b <= bhi; b++) {
+                bin_cell[b] = (u32)std::min<u64>(cells, 0xffffffffu);
+                cells += tiles;
+            }
+        }
+        bin_cell[nbins] = (u32)std::min<u64>(cells, 0xffffffffu);
+    }
+    p.msd = stiles > 0 && nbins <= SORT_MAX_BINS && cells <= SORT_MAX_CELLS;
     if (p.msd) {
         p.nbins = (u32)nbins;
         p.sort_tiles = (u32)stiles;
-        p.cnt_pad = (u32)align_up(nbins * stiles, SCAN_TILE);
+        p.ncells = (u32)cells;
+        p.cnt_pad = (u32)align_up(cells, SCAN_TILE);
         p.cscan_tiles = p.cnt_pad / SCAN_TILE;
         p.segcap = (u32)((entries + SEG_ENTRIES - 1) / SEG_ENTRIES + nbins);
     }
@@ -260,13 +287,15 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     p.win_off = align_up(sizeof(MsmDesc) * p.M, 16);
     p.blk_off = p.win_off + align_up(sizeof(WinDesc) * wins.size(), 16);
     p.tf_off = p.blk_off + align_up(sizeof(uint2) * rblocks.size(), 16);
-    p.tree_off = p.tf_off + align_up(sizeof(u32) * (p.M + 1), 16);
+    p.bc_off = p.tf_off + align_up(sizeof(u32) * (p.M + 1), 16);
+    p.tree_off = p.bc_off + align_up(sizeof(u32) * (p.msd ? p.nbins + 1 : 0), 16);
     const size_t tbytes = align_up(p.tree_off + sizeof(TreeGroup) * groups.size(), 256);
     p.tables.assign(tbytes, 0);
     std::memcpy(p.tables.data() + p.desc_off, descs.data(), sizeof(MsmDesc) * p.M);
     std::memcpy(p.tables.data() + p.win_off, wins.data(), sizeof(WinDesc) * wins.size());
     std::memcpy(p.tables.data() + p.blk_off, rblocks.data(), sizeof(uint2) * rblocks.size());
     std::memcpy(p.tables.data() + p.tf_off, tile_first.data(), sizeof(u32) * (p.M + 1));
+    if (p.msd) std::memcpy(p.tables.data() + p.bc_off, bin_cell.data(), sizeof(u32) * (p.nbins + 1));
     std::memcpy(p.tables.data() + p.tree_off, groups.data(), sizeof(TreeGroup) * groups.size());
 
     // device scratch layout
@@ -284,7 +313,7 @@ bool Plan::build(Plan &p, int device, const std::vector<MsmShape> &shapes) {
     lo.o_offsets = take((size_t)(p.nb + 1) * 4);
     lo.o_tiles = take(p.msd ? 0 : (size_t)(p.ntiles + 1) * 4);
     lo.o_entries = take((size_t)std::max<u64>(entries, 1) * 4);
-    const size_t ncnt = (size_t)p.nbins * p.sort_tiles;
+    const size_t ncnt = p.ncells;
     lo.o_cnt = take(p.msd ? (size_t)p.cnt_pad * 4 : 0);
     lo.o_coff = take(p.msd ? (ncnt + 1) * 4 : 0);
     lo.o_ccur = take(p.msd ? ncnt * 4 : 0);
@@ -464,8 +493,10 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
         u32 *coff = reinterpret_cast<u32 *>(sb + layout.o_coff);
         u32 *ccur = reinterpret_cast<u32 *>(sb + layout.o_ccur);
         u32 *ctiles = reinterpret_cast<u32 *>(sb + layout.o_ctiles);
-        const u32 ncnt = nbins * sort_tiles;
-        SortArgs sa{p.desc, p.tile_first, M, sort_tiles, tile_scalars, nbins, nb, segcap, cnt, coff,
+        const u32 ncnt = ncells;
+        const unsigned char *img = d_image ? static_cast<const unsigned char *>(d_image) : sb + layout.o_tables;
+        SortArgs sa{p.desc, p.tile_first, reinterpret_cast<const u32 *>(img + bc_off), M, sort_tiles, tile_scalars,
+                    nbins, nb, segcap, cnt, coff,
                     reinterpret_cast<u32 *>(sb + layout.o_centry),
                     reinterpret_cast<unsigned short *>(sb + layout.o_cfine),
                     reinterpret_cast<uint4 *>(sb + layout.o_segs), reinterpret_cast<uint2 *>(sb + layout.o_binseg),

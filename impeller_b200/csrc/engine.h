@@ -131,7 +131,7 @@ class Plan {
     u32 hist_grid_x = 1;
     // two-level sort (msd) or per-entry atomic bucket sort
     bool msd = false;
-    u32 nbins = 0, sort_tiles = 0, tile_scalars = 0, segcap = 0, cnt_pad = 0, cscan_tiles = 0;
+    u32 nbins = 0, sort_tiles = 0, tile_scalars = 0, segcap = 0, cnt_pad = 0, cscan_tiles = 0, ncells = 0;
     std::vector<MsmShape> shapes;
     PlanLayout layout{};
 
@@ -159,7 +159,7 @@ class Plan {
     size_t ext_cap = 0;
     cudaEvent_t staged = nullptr;
     std::vector<unsigned char> tables;  // host image of the tables
-    size_t desc_off = 0, win_off = 0, blk_off = 0, tf_off = 0, tree_off = 0;
+    size_t desc_off = 0, win_off = 0, blk_off = 0, tf_off = 0, bc_off = 0, tree_off = 0;
     u32 nwins = 0, nrblocks = 0;
     std::vector<u32> tree_first;  // reduction tree: first group of each level (+ total)
     bool profiling = false;

@@ -204,9 +204,11 @@ static_assert(FINE == FINE_BLOCK, "k_seg_scatter gives every bucket of a bin one
 struct SortArgs {
     const MsmDesc *descs;
     const u32 *tile_first;  // M + 1: first sort tile of each MSM
+    const u32 *bin_cell;    // nbins + 1: first count cell of each bin; [nbins] = cells
     u32 M, ntiles, tile_scalars, nbins, nb, segcap;
-    u32 *cnt;               // nbins x ntiles, bin-major (scan input, padded)
-    const u32 *coff;        // exclusive scan of cnt; coff[nbins * ntiles] = E
+    u32 *cnt;               // per MSM (bins on FINE boundaries), its bins x its tiles,
+                            // bin-major: cell bin_cell[b] + (tile - tile_first[m]) (scan input, padded)
+    const u32 *coff;        // exclusive scan of cnt; coff[bin_cell[nbins]] = E
     u32 *c_entry;           // entries in coarse order
     unsigned short *c_fine; // their bucket index within the bin
     uint4 *segs;            // per segment: bin, first, end
@@ -267,9 +269,11 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
     u32 m, start, end;
     sort_tile(a, blockIdx.x, m, start, end);
     const MsmDesc d = a.descs[m];
-    for (u32 b = threadIdx.x; b < a.nbins; b += blockDim.x) hist[b] = 0;
-    __syncthreads();
     const u32 B = 1u << (d.c - 1);
+    // this MSM's bins
+    const u32 blo = d.bucket_base >> FINE_BITS, bhi = (d.bucket_base + d.n_windows * B - 1u) >> FINE_BITS;
+    for (u32 b = blo + threadIdx.x; b <= bhi; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
     // the tile's keys, window-major: key of window w, scalar i at w * (end - start) + i - start
     const u32 tile_n = end - start;
     u32 *kp = a.keys + d.entry_base + (size_t)start * d.n_logical;
@@ -291,7 +295,8 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_coarse_count(SortArgs a) {
         });
     }
     __syncthreads();
-    for (u32 b = threadIdx.x; b < a.nbins; b += blockDim.x) a.cnt[(size_t)b * a.ntiles + blockIdx.x] = hist[b];
+    const u32 tl = blockIdx.x - a.tile_first[m];
+    for (u32 b = blo + threadIdx.x; b <= bhi; b += blockDim.x) a.cnt[a.bin_cell[b] + tl] = hist[b];
 }
 
 // Shared memory: delta[nbins], cur[nbins], stage_e[STAGE_ENTRIES] (u32),
@@ -316,15 +321,16 @@ __global__ void __launch_bounds__(SORT_BLOCK, 2) k_coarse_scatter(SortArgs a) {
     // distance from a local slot to the global coarse position
     const u32 per = (bhi - blo + blockDim.x) / blockDim.x;
     const u32 b0 = blo + threadIdx.x * per;
+    const u32 tl = tile - a.tile_first[m];
     u32 sum = 0;
     for (u32 k = 0; k < per; k++)
-        if (b0 + k <= bhi) sum += a.cnt[(size_t)(b0 + k) * a.ntiles + tile];
+        if (b0 + k <= bhi) sum += a.cnt[a.bin_cell[b0 + k] + tl];
     u32 total;
     u32 run = block_scan_excl(sum, total, warp_tot);
     for (u32 k = 0; k < per; k++) {
         const u32 b = b0 + k;
         if (b <= bhi) {
-            const size_t ci = (size_t)b * a.ntiles + tile;
+            const size_t ci = a.bin_cell[b] + tl;
             cur[b] = run;
             delta[b] = a.coff[ci] - run;
             run += a.cnt[ci];
@@ -382,7 +388,7 @@ __global__ void __launch_bounds__(FINE_BLOCK) k_seg_plan(SortArgs a) {
     for (u32 k = 0; k < per; k++) {
         const u32 b = b0 + k;
         if (b < a.nbins) {
-            const u32 size = a.coff[(size_t)(b + 1) * a.ntiles] - a.coff[(size_t)b * a.ntiles];
+            const u32 size = a.coff[a.bin_cell[b + 1]] - a.coff[a.bin_cell[b]];
             sum += (size + SEG_ENTRIES - 1) / SEG_ENTRIES;
         }
     }
@@ -391,7 +397,7 @@ __global__ void __launch_bounds__(FINE_BLOCK) k_seg_plan(SortArgs a) {
     for (u32 k = 0; k < per; k++) {
         const u32 b = b0 + k;
         if (b < a.nbins) {
-            const u32 bs = a.coff[(size_t)b * a.ntiles], be = a.coff[(size_t)(b + 1) * a.ntiles];
+            const u32 bs = a.coff[a.bin_cell[b]], be = a.coff[a.bin_cell[b + 1]];
             const u32 ns = (be - bs + SEG_ENTRIES - 1) / SEG_ENTRIES;
             a.bin_seg[b] = make_uint2(run, ns);
             for (u32 j = 0; j < ns; j++)
@@ -449,7 +455,7 @@ __global__ void __launch_bounds__(FINE_BLOCK) k_bin_scan(SortArgs a) {
     __shared__ u32 warp_tot[32];
     const u32 b = blockIdx.x;
     const uint2 bs = a.bin_seg[b];
-    const u32 base = a.coff[(size_t)b * a.ntiles];
+    const u32 base = a.coff[a.bin_cell[b]];
     u32 carry = base;
     for (u32 f0 = 0; f0 < FINE; f0 += blockDim.x) {
         const u32 f = f0 + threadIdx.x;
@@ -467,7 +473,7 @@ __global__ void __launch_bounds__(FINE_BLOCK) k_bin_scan(SortArgs a) {
         }
         carry += total;
     }
-    if (b == a.nbins - 1 && threadIdx.x == 0) a.offsets[a.nb] = a.coff[(size_t)a.nbins * a.ntiles];
+    if (b == a.nbins - 1 && threadIdx.x == 0) a.offsets[a.nb] = a.coff[a.bin_cell[a.nbins]];
 }
 
 // Shared memory: lcur[FINE], delta[FINE], stage_e[SEG_ENTRIES],
