@@ -569,10 +569,11 @@ cudaError_t Plan::run_front(void *scratch, const u32 *points, cudaStream_t st, b
     MARK(5);
 
     const u32 T = accum_blocks * accum_block;
-    FixupArgs fa{p.offsets, nb, T, p.recb, p.recp, buckets, p.longl, long_cap};
+    FixupArgs fa{p.offsets, nb, T, p.recb, p.recp, buckets, p.longl, long_cap, FIXUP_WARP_MAX};
     CURVE_LAUNCH(curve, k_fixup_short, (T + 255) / 256, 256, 0, st, fa);
     CK_LAUNCH("k_fixup_short");
-    CURVE_LAUNCH(curve, k_fixup_long, (u32)sm_count(device), 256, 0, st, fa);
+    const u32 wide_blocks = (u32)sm_count(device);
+    CURVE_LAUNCH(curve, k_fixup_long, wide_blocks + (u32)sm_count(device) * 2, WIDE_BLOCK, 0, st, fa, wide_blocks);
     CK_LAUNCH("k_fixup_long");
     MARK(6);
     return cudaSuccess;

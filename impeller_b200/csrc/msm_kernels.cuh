@@ -749,6 +749,12 @@ __global__ void __launch_bounds__(AccumShape<C>::threads, AccumShape<C>::per_sm)
     }
 }
 
+// Long runs of up to this many pieces are merged by one warp (pieces / 32
+// additions per lane, then a 5-step warp sum), longer ones by a block.
+#ifndef FIXUP_WARP_MAX
+#define FIXUP_WARP_MAX 256
+#endif
+
 struct FixupArgs {
     const u32 *offsets;
     u32 nb;
@@ -758,6 +764,7 @@ struct FixupArgs {
     u32 *buckets;
     u32 *long_list;      // [0] = count, then owner thread ids
     u32 long_cap;
+    u32 warp_max;        // longest run k_fixup_long gives one warp (0: every run)
 };
 
 // Owner of a cut bucket = the slice where the bucket begins (record 2t+1).
@@ -782,19 +789,59 @@ __global__ void k_fixup_short(FixupArgs f) {
     xyzz_store(f.buckets + (size_t)b * C::XW, acc);
 }
 
-// One warp per long run (a bucket spread over more than 5 slices).
+// Long runs (a bucket spread over more than 5 slices), in one launch:
+// blocks below wide_blocks take the runs of more than warp_max pieces, one
+// 128-thread block per run (every thread one piece, more only past 128;
+// then a warp sum and a sum of the warps' sums: log2 of the run's length
+// deep); the other blocks' warps take the shorter runs, one warp per run
+// (pieces / 32 additions per lane, then a 5-step warp sum).  Both kinds run
+// at the same time.  wide_blocks == 0 or warp_max == 0: every run by a warp.
+static constexpr u32 WIDE_BLOCK = 128;
 template <class C>
-__global__ void k_fixup_long(FixupArgs f) {
+__global__ void k_fixup_long(FixupArgs f, u32 wide_blocks) {
     using FQ = typename C::Fq;
-    const u32 lane = threadIdx.x & 31u;
-    const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
+    __shared__ __align__(16) u32 part[WIDE_BLOCK / 32][C::XW];
+    const u32 lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     const u32 count = min(f.long_list[0], f.long_cap);
     const u32 E = f.offsets[f.nb];
     const u32 L = (E + f.T - 1) / f.T;
-    for (u32 w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += nwarps) {
+    const u32 wmax = f.warp_max && wide_blocks ? f.warp_max : 0xffffffffu;
+    if (blockIdx.x < wide_blocks) {
+        for (u32 w = blockIdx.x; w < count; w += wide_blocks) {  // the same runs for the whole block
+            const u32 t = f.long_list[1 + w];
+            const u32 b = f.rec_bucket[2 * t + 1];
+            const u32 pieces = (f.offsets[b + 1] - 1) / L - t + 1;  // the owner's, then slices t+1 ..
+            if (pieces <= wmax) continue;
+            XyzzT<FQ> acc = xyzz_identity<FQ>();
+            for (u32 k = threadIdx.x; k < pieces; k += WIDE_BLOCK) {
+                const size_t slot = k == 0 ? 2 * (size_t)t + 1 : 2 * (size_t)(t + k);
+                acc = xyzz_add(acc, xyzz_load<FQ>(f.rec_point + slot * C::XW));
+            }
+            const u32 nw = min((pieces + 31) / 32, WIDE_BLOCK / 32);  // warps holding pieces
+            if (wid < nw) {
+#pragma unroll 1
+                for (u32 o = 16; o; o >>= 1) acc = xyzz_add(acc, xyzz_shfl_down(acc, o));
+                if (lane == 0) xyzz_store(&part[wid][0], acc);
+            }
+            __syncthreads();
+            if (wid == 0) {
+                XyzzT<FQ> v = lane < nw ? xyzz_load<FQ>(&part[lane][0]) : xyzz_identity<FQ>();
+                u32 P = 1;
+                while (P < nw) P <<= 1;
+#pragma unroll 1
+                for (u32 o = P >> 1; o; o >>= 1) v = xyzz_add(v, xyzz_shfl_down(v, o));
+                if (lane == 0) xyzz_store(f.buckets + (size_t)b * C::XW, v);
+            }
+            __syncthreads();  // part is reused by the block's next run
+        }
+        return;
+    }
+    const u32 nwarps = ((gridDim.x - wide_blocks) * blockDim.x) >> 5;
+    for (u32 w = ((blockIdx.x - wide_blocks) * blockDim.x + threadIdx.x) >> 5; w < count; w += nwarps) {
         const u32 t = f.long_list[1 + w];
         const u32 b = f.rec_bucket[2 * t + 1];
         const u32 t1 = (f.offsets[b + 1] - 1) / L;
+        if (t1 - t + 1 > wmax) continue;  // a wide block's
         XyzzT<FQ> acc = xyzz_identity<FQ>();
         if (lane == 0) acc = xyzz_load<FQ>(f.rec_point + (size_t)(2 * t + 1) * C::XW);
         for (u32 s = t + 1 + lane; s <= t1; s += 32)
@@ -804,6 +851,7 @@ __global__ void k_fixup_long(FixupArgs f) {
         if (lane == 0) xyzz_store(f.buckets + (size_t)b * C::XW, acc);
     }
 }
+
 
 // ----------------------------------------------------------------- reduce
 //

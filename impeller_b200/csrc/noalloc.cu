@@ -219,7 +219,7 @@ extern "C" cudaError_t impeller_msm_device_noalloc(const uint32_t *d_points, con
     FixupArgs fa{offsets, NB, T, recb, recp, buckets, longl, T};
     K::k_fixup_short<K::Bn254><<<T / 256, 256, 0, stream>>>(fa);
     NA_LAUNCHED("k_fixup_short");
-    K::k_fixup_long<K::Bn254><<<64, 256, 0, stream>>>(fa);
+    K::k_fixup_long<K::Bn254><<<64, 256, 0, stream>>>(fa, 0u);
     NA_LAUNCHED("k_fixup_long");
     ReduceArgs ra{wins, rblk, offsets, buckets, parts_v, parts_s};
     K::k_reduce<K::Bn254><<<NRBLOCKS, K::REDUCE_BLOCK, 0, stream>>>(ra);
