@@ -85,6 +85,24 @@ def test_c3_skewed_full_size(M):
     ctx.close()
 
 
+def test_many_heavy_buckets(M):
+    """2^20 scalars taking 200 small values: 200 buckets of window 0 each cut
+    into more than 256 slices, more heavy buckets than the fixup has blocks
+    (so a block merges several, one after another), with plain windows and
+    with window 8."""
+    n = 1 << 20
+    dp = M.gen_points_device(n, seed=5)
+    h = M.to_host(dp).reshape(n, 16)
+    vals = np.stack([O.int_to_limbs(O.to_mont(v, O.R_MOD)) for v in range(1, 201)])
+    sc = vals[np.arange(n) % 200]
+    want = O.msm(h, sc)
+    ctx = M.MsmContext(dp)
+    dsc = M.to_device(sc)
+    for c in (0, 8):
+        assert (M.to_host(ctx.msm_device(dsc, c=c)) == want).all(), c
+    ctx.close()
+
+
 def test_c4_batched_every_output(M):
     n = 1 << 20
     dp = M.gen_points_device(n, seed=0)
