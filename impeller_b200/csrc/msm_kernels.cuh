@@ -174,11 +174,13 @@ __global__ void k_scatter(const MsmDesc *__restrict__ descs, u32 *__restrict__ c
 // two-level sort keeps every atomic in shared memory and every global write
 // in runs:
 //   k_coarse_count    per tile of scalars: entries per coarse bin (the top
-//                     bits of the global bucket index; FINE buckets per bin)
-//   (scan)            bin-major exclusive scan of the tile counts
-//   k_coarse_scatter  per tile: entries staged in shared memory in bin order,
-//                     written out as one contiguous run per bin, with the
-//                     fine index (bucket within the bin) beside them
+//                     bits of the global bucket index; FINE buckets per bin),
+//                     and every digit's bucket key for the scatter
+//   (scan)            bin-major exclusive scan of the tile counts (per MSM
+//                     its own bins x its own tiles)
+//   k_coarse_scatter  per tile: the keys' entries staged in shared memory in
+//                     bin order, written out as one contiguous run per bin,
+//                     with the fine index (bucket within the bin) beside them
 //   k_seg_plan        split every bin into segments of at most SEG_ENTRIES
 //   k_seg_hist        per segment: entries per fine bucket
 //   k_bin_scan        per bin: bucket offsets, and each segment's cursor per
