@@ -70,6 +70,19 @@ def test_window_table_roundtrip(L):
     M.restore_default_window_table()
 
 
+def test_compiled_table_matches_autotune_json(L):
+    """The library's built-in window table is the committed measurement
+    (impeller_b200/autotune_table.json, compiled in at build time)."""
+    import json
+    import os
+    M.restore_default_window_table()
+    path = os.path.join(os.path.dirname(M.__file__), "autotune_table.json")
+    for e in json.load(open(path))["entries"]:
+        n = 1 << e["log2n"]
+        assert M.default_window(n) == e["plain_c"], e
+        assert M.table_window(n) == (e.get("tables_c") or 0), e
+
+
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(lib.ImpellerError):
         lib.load(str(tmp_path / "libimpeller_msm.so"))
